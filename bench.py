@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Throughput of the Kelvin–Helmholtz step (cell-steps/s) on B200.
+
+Workload (default): the plain single large run, 4096 x 8192 — NZ = 4096
+cells along the periodic flow axis (Lz = 2 pi) by NX = 8192 along the shear
+axis (Lx = 20) — FP64, V0 = 0.05, shear width 1, kz = 1 seed of amplitude
+0.15 V0 on Az2/Az3 (run_mode 6), alpha = 1, CFL 0.4.  Synthetic: the
+initial state is the reference's analytic equilibrium plus seed.
+
+Filter: the reference's band-filter kernels launch one thread per z cell
+and cannot launch for NZ > 1024 (ymgpu2d/main_ym.cu:396, YM_Physics.cu:349),
+so the reference's own step at this size performs no filtering; the default
+``--filter ref`` reproduces that.  ``--filter keep`` subtracts modes above
+NZ/3 every step with the dense FP64 contraction (reported under
+``filter_keep`` when ``--with-filter-line`` is given).
+
+One step = one iteration of the reference loop over the whole grid.  The
+state (12.9 GB for two buffers) is far larger than L2 (126 MB), so no flush
+is needed between steps.  N > 1: independent replicas, one per GPU (the
+path does not shard across GPUs), ``scaling: weak``.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    # name: (NX shear, NZ periodic)
+    "kh_4096x8192": (8192, 4096),
+    "kh_256x512": (512, 256),
+    # profiling size: 805 MB per state buffer (> L2), for ncu captures
+    "kh_1024x2048": (2048, 1024),
+}
+PHYSICS = ("k_mode = 1\nalpha_YM = 1.0\nperturb_amp = 0.15\nrun_mode = 6\nV0 = 0.05\neps_override = 1.0\n"
+           "lx_override = 20\ncourant_override = 0.4\n")
+BYTES_STEP = 376  # compulsory: read 24 FP64 arrays, write 23 (Az1 frozen)
+BYTES_FCT = 288   # fct_fused_kernel: read 12 fluid + 12 field arrays, write 12 fluid
+BYTES_MAXWELL = 280  # maxwell_fused_kernel: read 24, write 11 (Az1 frozen)
+
+
+def ini_for(workload: str, filt: str) -> str:
+    nx, nz = WORKLOADS[workload]
+    text = PHYSICS + f"nx_override = {nx}\nnz_override = {nz}\n"
+    if filt == "keep" or (filt == "ref" and nz <= 1024):
+        text += f"kz_keep_max = {nz // 3}\n"
+    return text
+
+
+def measured_peaks() -> tuple:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.lines: list[str] = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.idx)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device(f"cuda:{local}"))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_oracle_rate(workload: str, steps: int, threads: int | None = None) -> dict:
+    """The FP64 OpenMP oracle on a bounded sample of the workload: the full
+    shear extent and NZ reduced to 256 rows (the step's per-cell work does not
+    depend on NZ when no band filter runs)."""
+    import numpy as np
+
+    from kh_simulations_b200._lib import Grid
+    from kh_simulations_b200.config import derive, loads, step_params
+    from oracle import Oracle
+
+    if threads:
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+    nx, _ = WORKLOADS[workload]
+    nz = 256
+    cfg = loads(PHYSICS + f"nx_override = {nx}\nnz_override = {nz}\n")
+    d = derive(cfg)
+    g = Grid(d.nx, d.nz, d.dx, d.dz)
+    p = step_params(cfg, d)
+    orc = Oracle()
+    st = np.zeros((24, nz, nx))
+    st[12] = st[18] = 1.0
+    st[15], st[21] = 1.0, -1.0
+    x = np.arange(nx)
+    xi = (x * d.dx - nx * d.dx * 0.5) / d.eps
+    st[14] = d.V0 * np.tanh(xi)[None, :]
+    st[20] = -st[14]
+    orc.step(g, p, st, 1)  # warm-up (page-in, thread pool)
+    t0 = time.perf_counter()
+    orc.step(g, p, st, steps)
+    dt = time.perf_counter() - t0
+    return {"value": nx * nz * steps / dt, "unit": "cell-steps/s", "cores": orc.threads(), "kind": "port",
+            "sample": f"FP64 OpenMP oracle, {steps} step(s) of the same physics on {nz}x{nx} (NZ x NX) = "
+                      f"{nx * nz} cells, no band filter, {dt:.2f} s"}
+
+
+def run_reference(args, world, rank, local):
+    """Reference arm: the reference's own step on the host cores (it has no
+    CPU implementation, so this is the FP64 OpenMP port), plus the
+    reference's own CUDA kernels timed on this GPU when the harness is built."""
+    if rank != 0:
+        return 0
+    per = []
+    cb = None
+    for k in range(args.warmup + args.steps):
+        r = cpu_oracle_rate(args.workload, 1)
+        if k >= args.warmup:
+            per.append(r["value"])
+            cb = r
+    value = statistics.median(per)
+    line = {"metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "filter": "none (reference cannot launch its band filter "
+                       "for NZ > 1024)"},
+            "cpu_baseline": {**cb, "value": value},
+            "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    try:
+        line["reference_cuda"] = ref_cuda_rate(args)
+    except Exception as e:  # the CPU arm stands on its own
+        line["reference_cuda"] = {"unavailable": str(e)[:200]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def ref_cuda_rate(args) -> dict:
+    """The reference's own kernels (oracle/_ref/libymref.so, its stock
+    flags) through its own stage sequence, timed with CUDA events."""
+    import torch
+
+    from kh_simulations_b200._lib import Grid
+    from kh_simulations_b200.config import derive, loads, step_params
+    from kh_simulations_b200.run import init_params
+    from oracle import REF_STOCK_LIB, RefHarness
+
+    if not torch.cuda.is_available() or not REF_STOCK_LIB.exists():
+        raise RuntimeError("no GPU or reference harness not built")
+    cfg = loads(ini_for(args.workload, "ref"))
+    d = derive(cfg)
+    ref = RefHarness(parity=False)
+    ref.create(Grid(d.nx, d.nz, d.dx, d.dz), step_params(cfg, d))
+    ip, _k = init_params(cfg, d)
+    ref.init(ip)
+    ref.step(max(1, args.warmup))
+    ms = ref.time_steps(args.steps)
+    ref.destroy()
+    cells = d.nx * d.nz
+    return {"value": cells * args.steps / (ms / 1e3), "unit": "cell-steps/s", "ms_per_step": ms / args.steps,
+            "build": "reference sources unmodified, nvcc -O2 sm_100a (its stock flags)"}
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="kh_4096x8192")
+    ap.add_argument("--filter", choices=["ref", "keep"], default="ref")
+    ap.add_argument("--with-filter-line", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        return run_reference(args, world, rank, local)
+
+    import torch
+
+    from kh_simulations_b200 import _lib
+    from kh_simulations_b200.config import loads
+    from kh_simulations_b200.run import KHRun
+
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    cfg = loads(ini_for(args.workload, args.filter))
+    run = KHRun(cfg, device=dev)
+    run.init()
+    d = run.d
+    cells = d.nx * d.nz
+    stream = torch.cuda.Stream(device=dev)
+    run.step(args.warmup, stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+
+    sampler = ClockSampler(dev.index if dev.index is not None else 0)
+    sampler.start()
+    time.sleep(0.3)
+    l0 = _lib.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    run.step(args.steps, stream)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    launches = _lib.launch_count() - l0
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(ms, world)
+    barrier(world)
+    value = cells * args.steps * world / (ms_max / 1e3)
+
+    # per-stage device times (separate uncaptured pass, events between stages)
+    nst = 3
+    out = (C.c_float * 8)()
+    _lib.check(_lib.load().ymkh_stage_times(run.ctx, nst, C.c_void_p(stream.cuda_stream), out, 8), "stage times")
+    stage_ms = {n: out[i] / nst for i, n in enumerate(_lib.STAGES)}
+    dom = max(stage_ms, key=stage_ms.get)
+    peak, peak_kind = measured_peaks()
+    alg = {"fct": BYTES_FCT, "maxwell": BYTES_MAXWELL}.get(dom)
+    roof = None
+    if alg is not None:
+        achieved = alg * cells / (stage_ms[dom] / 1e3) / 1e9
+        traffic = None
+        tf = ROOT / "profiles" / "traffic.json"
+        if tf.exists():
+            t = json.loads(tf.read_text()).get(dom)
+            if t:
+                traffic = t * cells
+        roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                "algorithmic_bytes_per_cell": alg}
+    step_gbs = BYTES_STEP * cells / (ms / args.steps / 1e3) / 1e9
+
+    line = {"metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "nz_periodic": d.nz, "nx_shear": d.nx,
+                       "filter": "keep |k| <= NZ/3" if d.bands else "none (as the reference at NZ > 1024)",
+                       "l2": "state 12.9 GB >> L2; no flush needed", "parallelism": f"replicas x{world}",
+                       "graph_steps": 4},
+            "roofline": roof,
+            "step_roofline": {"bytes_per_cell_step": BYTES_STEP, "achieved": step_gbs, "peak": peak,
+                              "frac": step_gbs / peak, "unit": "GB/s"},
+            "stage_ms": stage_ms, "clocks": clocks, "gpu_launches": launches}
+
+    if not args.no_e2e:
+        line["e2e"] = e2e_rate(run, args, stream, world)
+    run.close()
+    del run
+    torch.cuda.empty_cache()
+
+    if args.with_filter_line and args.filter == "ref" and d.nz > 1024:
+        line["filter_keep"] = filter_keep_rate(args, dev)
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_oracle_rate(args.workload, 1)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def e2e_rate(run, args, stream, world) -> dict:
+    """Same metric through the public API with host buffers: upload the
+    state from pinned host memory, K steps each followed by the energy
+    read back (the reference's per-step diagnostic), download the state."""
+    import torch
+
+    st_host = run.state.to("cpu").pin_memory()
+    out_host = torch.empty_like(st_host).pin_memory()
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        run.buf[0].copy_(st_host, non_blocking=True)
+    run.lib.ymkh_set_current_buffer(run.ctx, 0)
+    for _ in range(args.steps):
+        run.step(1, stream)
+        run.energy(stream)
+    with torch.cuda.stream(stream):
+        out_host.copy_(run.state, non_blocking=True)
+    stream.synchronize()
+    dt = time.perf_counter() - t0
+    dt = max_over_ranks(dt, world)
+    cells = run.d.nx * run.d.nz
+    sb = st_host.numel() * 8
+    return {"value": cells * args.steps * world / dt, "unit": "cell-steps/s",
+            "h2d_bytes_per_step": sb / args.steps, "d2h_bytes_per_step": 8 + sb / args.steps,
+            "note": "state uploaded once and downloaded once per K-step call; energy read back every step"}
+
+
+def filter_keep_rate(args, dev) -> dict:
+    import torch
+
+    from kh_simulations_b200.config import loads
+    from kh_simulations_b200.run import KHRun
+
+    cfg = loads(ini_for(args.workload, "keep"))
+    run = KHRun(cfg, device=dev)
+    run.init()
+    stream = torch.cuda.Stream(device=dev)
+    run.step(2, stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    n = 2
+    e0.record(stream)
+    run.step(n, stream)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / n
+    cells = run.d.nx * run.d.nz
+    run.close()
+    return {"value": cells / (ms / 1e3), "unit": "cell-steps/s", "ms_per_step": ms,
+            "bands": run.d.bands}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

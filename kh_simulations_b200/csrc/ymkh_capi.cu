@@ -1,0 +1,531 @@
+// ymkh_capi.cu — the extern "C" boundary of include/ymkh.h: context
+// lifetime, state binding, the step sequence and the diagnostics.
+//
+// The step keeps the reference's stage order (ymgpu2d/main_ym.cu:324-455):
+//   FCT x+z sweeps of both beams, density floor   -> fct_fused_kernel
+//   currents, Ampère, potential, Faraday          -> maxwell_fused_kernel
+//   sponge, xi_cut                                -> sponge_xicut_kernel
+//   z-mean removal                                -> zmean_kernel
+//   DFT kz bands on the 21 filtered arrays        -> band_coef / band_apply
+//   z-hyperdiffusion                              -> hyperdiff_kernel
+//   colour-1 EM zeroing                           -> cudaMemsetAsync
+// The sources of stage 7 are recomputed inside the next FCT launch.
+//
+// The stencil kernels read start-of-step values of neighbouring tiles, so
+// the state alternates between two 24-array buffers: buffer 0 is the state
+// the caller binds; buffer 1 is either a second caller-bound set
+// (ymkh_bind_state2, zero copy) or allocated here once.  With a library
+// buffer, ymkh_step copies back when it ends on buffer 1, so the caller's
+// arrays always hold the current state after the call.
+
+#include <cstdio>
+#include <cstring>
+#include <cstdarg>
+#include <atomic>
+#include <vector>
+#include <algorithm>
+#include "ymkh_common.cuh"
+
+
+using namespace ymkh;
+
+namespace {
+
+thread_local int t_err_code = 0;
+thread_local char t_err_msg[512] = "";
+std::atomic<long long> g_launches{0};
+
+int set_err(int code, const char* fmt, ...) {
+  t_err_code = code;
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(t_err_msg, sizeof t_err_msg, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CK(call, what)                                                                    \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess) return set_err(YMKH_ECUDA, "%s: %s", what, cudaGetErrorString(e_)); \
+  } while (0)
+
+constexpr int MAX_BANDS = 2 + YMKH_MAX_EXTRA_BANDS;
+
+}  // namespace
+
+struct ymkh_ctx {
+  int device = 0;
+  int nx = 0, nz = 0;
+  size_t N = 0;
+  ymkh_params prm{};
+  StepParams sp{};
+  State buf[2]{};
+  bool bound = false;
+  bool dual = false;         // second buffer bound by the caller
+  double* own = nullptr;     // library second buffer (24*N doubles)
+  int cur = 0;
+  int nb = 0, lo[MAX_BANDS]{}, hi[MAX_BANDS]{}, J[MAX_BANDS]{};
+  double* W[MAX_BANDS]{};
+  double* coef = nullptr;    // band coefficients [21][J][nx]
+  double* epart = nullptr;   // energy partials
+  double* edev = nullptr;    // [0] energy, [1..2] mode amplitudes
+  double* mcol = nullptr;    // mode amplitude per-column buffer
+  int fct_tx = 64, fct_seg = 16;
+  // CUDA graphs of `graph_steps` steps, one per starting buffer
+  int graph_steps = 4;
+  cudaGraphExec_t gexec[2]{nullptr, nullptr};
+  cudaStream_t gstream[2]{nullptr, nullptr};
+  long long glaunches[2]{0, 0};  // kernels per captured graph
+  // optional per-stage event timing (ymkh_stage_times)
+  cudaEvent_t ev[16]{};
+  int nev = 0;
+  bool timing = false;
+};
+
+namespace {
+
+void fill_step_params(ymkh_ctx* c) {
+  const ymkh_params& p = c->prm;
+  StepParams& s = c->sp;
+  s.nx = c->nx; s.nz = c->nz;
+  s.dx = p.dx; s.dz = p.dz; s.dt = p.dt_step;
+  s.c2 = p.c * p.c; s.eps0 = p.eps_0; s.alpha = p.alpha_YM;
+  s.freeze_az1 = p.freeze_az1; s.periodic_x = p.periodic_x;
+  s.epsilon = p.epsilon; s.xi_sponge = p.xi_sponge; s.sigma_sponge = p.sigma_sponge;
+  s.xi_cut = p.xi_cut; s.warm_T = p.warm_T; s.suppress_kz0 = p.suppress_kz0;
+  s.hyp_diff = p.hyp_diff_coeff;
+}
+
+int band_list(const ymkh_params& p, int* lo, int* hi) {
+  int n = 0;
+  if (p.kz_suppress_max >= 1) { lo[n] = 1; hi[n] = p.kz_suppress_max; ++n; }
+  if (p.kz_suppress_hi > p.kz_suppress_max + 1) { lo[n] = p.kz_suppress_max + 2; hi[n] = p.kz_suppress_hi; ++n; }
+  for (int i = 0; i < p.n_extra_bands && i < YMKH_MAX_EXTRA_BANDS; ++i) {
+    lo[n] = p.extra_band_lo[i]; hi[n] = p.extra_band_hi[i]; ++n;
+  }
+  return n;
+}
+
+void drop_graphs(ymkh_ctx* c) {
+  for (int k = 0; k < 2; ++k)
+    if (c->gexec[k]) { cudaGraphExecDestroy(c->gexec[k]); c->gexec[k] = nullptr; c->gstream[k] = nullptr; }
+}
+
+void free_bands(ymkh_ctx* c) {
+  for (int b = 0; b < MAX_BANDS; ++b) if (c->W[b]) { cudaFree(c->W[b]); c->W[b] = nullptr; }
+  if (c->coef) { cudaFree(c->coef); c->coef = nullptr; }
+  c->nb = 0;
+}
+
+int setup_params(ymkh_ctx* c, const ymkh_params* p) {
+  if (p->dt_step <= 0 || p->dx <= 0 || p->dz <= 0) return set_err(YMKH_EINVAL, "dx, dz, dt_step must be > 0");
+  if (p->filter_engine != YMKH_FILTER_DFT) return set_err(YMKH_EINVAL, "unknown filter_engine %d", p->filter_engine);
+  if (p->suppress_kz0 && (c->nz & (c->nz - 1)) != 0)
+    return set_err(YMKH_EINVAL, "suppress_kz0 requires NZ a power of 2 (got %d)", c->nz);
+  if (p->n_extra_bands < 0 || p->n_extra_bands > YMKH_MAX_EXTRA_BANDS)
+    return set_err(YMKH_EINVAL, "n_extra_bands out of range");
+  int lo[MAX_BANDS], hi[MAX_BANDS];
+  const int nb = band_list(*p, lo, hi);
+  for (int b = 0; b < nb; ++b)
+    if (lo[b] < 0 || hi[b] < lo[b] || hi[b] > 1 << 20) return set_err(YMKH_EINVAL, "bad band [%d, %d]", lo[b], hi[b]);
+  drop_graphs(c);
+  free_bands(c);
+  c->prm = *p;
+  fill_step_params(c);
+  size_t maxJ = 0;
+  for (int b = 0; b < nb; ++b) {
+    c->lo[b] = lo[b]; c->hi[b] = hi[b]; c->J[b] = 2 * (hi[b] - lo[b] + 1);
+    CK(cudaMalloc(&c->W[b], (size_t)c->nz * c->J[b] * sizeof(double)), "cudaMalloc twiddles");
+    CK(launch_twiddles(c->W[b], c->nz, lo[b], hi[b], c->J[b], 0), "twiddle kernel");
+    g_launches++;
+    maxJ = std::max(maxJ, (size_t)c->J[b]);
+  }
+  c->nb = nb;
+  if (nb) CK(cudaMalloc(&c->coef, 21 * maxJ * (size_t)c->nx * sizeof(double)), "cudaMalloc band coefficients");
+  CK(cudaDeviceSynchronize(), "twiddle setup");
+  return 0;
+}
+
+void choose_launch_shape(ymkh_ctx* c) {
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+  c->fct_tx = c->nx >= 64 ? 64 : 32;
+  const int strips = (c->nx + c->fct_tx - 1) / c->fct_tx;
+  const int target = 4 * sms;  // 2 CTAs per SM, two waves
+  int segs = std::max(1, (target + strips - 1) / strips);
+  int seg = (c->nz + segs - 1) / segs;
+  c->fct_seg = std::max(16, seg);
+}
+
+ArrayList list21(const State& s) {
+  ArrayList l{};
+  double* v[21] = {s.f[BY1], s.f[EX1], s.f[EZ1], s.f[BY2], s.f[BY3], s.f[EX2], s.f[EX3],
+                   s.f[EZ2], s.f[EZ3], s.f[AZ2], s.f[AZ3], s.a[FQ2], s.a[FQ3], s.b[FQ2],
+                   s.b[FQ3], s.a[FPZ], s.b[FPZ], s.a[FPX], s.b[FPX], s.a[FN], s.b[FN]};
+  for (int i = 0; i < 21; ++i) l.p[i] = v[i];
+  return l;
+}
+ArrayList list12(const State& s) {
+  ArrayList l{};
+  double* v[12] = {s.f[BY2], s.f[BY3], s.f[EX2], s.f[EX3], s.f[EZ2], s.f[EZ3],
+                   s.f[AZ2], s.f[AZ3], s.a[FQ2], s.a[FQ3], s.b[FQ2], s.b[FQ3]};
+  for (int i = 0; i < 12; ++i) l.p[i] = v[i];
+  return l;
+}
+
+// One reference iteration from buffer c->cur into buffer 1 - c->cur.
+enum Stage { ST_FCT = 0, ST_MAXWELL, ST_POINTWISE, ST_ZMEAN, ST_BANDS, ST_HYPER, ST_ZERO, ST_COUNT };
+
+void mark(ymkh_ctx* c, int stage, cudaStream_t s) {
+  if (c->timing) cudaEventRecord(c->ev[stage], s);
+}
+
+int step_once(ymkh_ctx* c, cudaStream_t s) {
+  const State& in = c->buf[c->cur];
+  const State& out = c->buf[1 - c->cur];
+  mark(c, ST_FCT, s);
+  CK(launch_fct(in, out, c->sp, c->fct_tx, c->fct_seg, s), "fct_fused_kernel");
+  mark(c, ST_MAXWELL, s);
+  CK(launch_maxwell(out, in, out, c->sp, s), "maxwell_fused_kernel");
+  mark(c, ST_POINTWISE, s);
+  g_launches += 2;
+  if (c->prm.xi_sponge > 0.0) { CK(launch_sponge_xicut(list12(out), c->sp, 0, s), "sponge"); g_launches++; }
+  if (c->prm.xi_cut > 0.0) { CK(launch_sponge_xicut(list12(out), c->sp, 1, s), "xi_cut"); g_launches++; }
+  mark(c, ST_ZMEAN, s);
+  if (c->prm.suppress_kz0) { CK(launch_zmean(list21(out), c->nx, c->nz, s), "zmean"); g_launches++; }
+  mark(c, ST_BANDS, s);
+  const double inv2 = (double)(2.0f / (float)c->nz);
+  for (int b = 0; b < c->nb; ++b) {
+    CK(launch_band(list21(out), 21, c->W[b], c->J[b], c->J[b], c->coef, c->nx, c->nz, inv2, s), "band filter");
+    g_launches += 2;
+  }
+  mark(c, ST_HYPER, s);
+  if (c->prm.hyp_diff_coeff > 0.0) {
+    CK(launch_hyperdiff(list12(out), c->nx, c->nz, c->prm.hyp_diff_coeff, s), "hyperdiffusion");
+    g_launches++;
+  }
+  mark(c, ST_ZERO, s);
+  if (c->prm.suppress_kz0) {
+    const size_t bytes = c->N * sizeof(double);
+    CK(cudaMemsetAsync(out.f[BY1], 0, bytes, s), "zero By1");
+    CK(cudaMemsetAsync(out.f[EX1], 0, bytes, s), "zero Ex1");
+    CK(cudaMemsetAsync(out.f[EZ1], 0, bytes, s), "zero Ez1");
+  }
+  mark(c, ST_COUNT, s);
+  c->cur = 1 - c->cur;
+  return 0;
+}
+
+int copy_back(ymkh_ctx* c, cudaStream_t s) {
+  const size_t bytes = c->N * sizeof(double);
+  const State& a = c->buf[1];
+  const State& b = c->buf[0];
+  for (int i = 0; i < 12; ++i) CK(cudaMemcpyAsync(b.f[i], a.f[i], bytes, cudaMemcpyDeviceToDevice, s), "copy back");
+  for (int i = 0; i < 6; ++i) {
+    CK(cudaMemcpyAsync(b.a[i], a.a[i], bytes, cudaMemcpyDeviceToDevice, s), "copy back");
+    CK(cudaMemcpyAsync(b.b[i], a.b[i], bytes, cudaMemcpyDeviceToDevice, s), "copy back");
+  }
+  c->cur = 0;
+  return 0;
+}
+
+int run_graph(ymkh_ctx* c, cudaStream_t s) {
+  const int start = c->cur;
+  if (!c->gexec[start] || c->gstream[start] != s) {
+    if (c->gexec[start]) { cudaGraphExecDestroy(c->gexec[start]); c->gexec[start] = nullptr; }
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+    int rc = 0;
+    const long long l0 = g_launches.load();
+    for (int k = 0; k < c->graph_steps && !rc; ++k) rc = step_once(c, s);
+    c->glaunches[start] = g_launches.load() - l0;
+    g_launches -= c->glaunches[start];  // counted when the graph runs
+    cudaError_t ec = cudaStreamEndCapture(s, &g);
+    c->cur = start;  // capture did not execute anything
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    CK(ec, "end capture");
+    cudaError_t ei = cudaGraphInstantiate(&c->gexec[start], g, 0);
+    cudaGraphDestroy(g);
+    CK(ei, "graph instantiate");
+    c->gstream[start] = s;
+  }
+  CK(cudaGraphLaunch(c->gexec[start], s), "graph launch");
+  g_launches += c->glaunches[start];
+  // graph_steps is even: the state ends in the buffer it started from
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ymkh_last_error(char* buf, size_t n) {
+  if (buf && n) {
+    strncpy(buf, t_err_msg, n - 1);
+    buf[n - 1] = 0;
+  }
+  return t_err_code;
+}
+
+long long ymkh_launch_count(void) { return g_launches.load(); }
+
+int ymkh_create(const ymkh_grid* grid, const ymkh_params* params, ymkh_ctx** out) {
+  if (!grid || !params || !out) return set_err(YMKH_EINVAL, "null argument");
+  if (grid->nx < 4 || grid->nz < 4) return set_err(YMKH_EINVAL, "grid too small (%d x %d)", grid->nx, grid->nz);
+  if ((size_t)grid->nx * grid->nz > ((size_t)1 << 34)) return set_err(YMKH_EINVAL, "grid too large");
+  ymkh_ctx* c = new ymkh_ctx();
+  CK(cudaGetDevice(&c->device), "cudaGetDevice");
+  c->nx = grid->nx; c->nz = grid->nz; c->N = (size_t)grid->nx * grid->nz;
+  int rc = setup_params(c, params);
+  if (rc) { free_bands(c); delete c; return rc; }
+  choose_launch_shape(c);
+  CK(prepare_fct(c->fct_tx), "FCT kernel attributes");
+  CK(prepare_column(c->nz), "column kernel attributes");
+  const int np = energy_nparts(c->N);
+  if (cudaMalloc(&c->epart, (size_t)2 * np * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->edev, 4 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->mcol, (size_t)2 * c->nx * sizeof(double)) != cudaSuccess) {
+    ymkh_destroy(c);
+    return set_err(YMKH_ENOMEM, "cudaMalloc diagnostics");
+  }
+  *out = c;
+  return 0;
+}
+
+int ymkh_set_params(ymkh_ctx* c, const ymkh_params* p) {
+  if (!c || !p) return set_err(YMKH_EINVAL, "null argument");
+  int rc = setup_params(c, p);
+  if (rc) return rc;
+  return 0;
+}
+
+static State make_state(double* const f[12], double* const a[6], double* const b[6]) {
+  State s{};
+  for (int i = 0; i < 12; ++i) s.f[i] = f[i];
+  for (int i = 0; i < 6; ++i) { s.a[i] = a[i]; s.b[i] = b[i]; }
+  return s;
+}
+
+static bool state_ok(const State& s) {
+  for (int i = 0; i < 12; ++i) if (!s.f[i]) return false;
+  for (int i = 0; i < 6; ++i) if (!s.a[i] || !s.b[i]) return false;
+  return true;
+}
+
+int ymkh_bind_state(ymkh_ctx* c, double* const fields[YMKH_NFIELDS], double* const fluidA[YMKH_NFLUID],
+                    double* const fluidB[YMKH_NFLUID]) {
+  if (!c || !fields || !fluidA || !fluidB) return set_err(YMKH_EINVAL, "null argument");
+  State s = make_state(fields, fluidA, fluidB);
+  if (!state_ok(s)) return set_err(YMKH_EINVAL, "null state array");
+  drop_graphs(c);
+  c->buf[0] = s;
+  if (!c->own) {
+    if (cudaMalloc(&c->own, 24 * c->N * sizeof(double)) != cudaSuccess)
+      return set_err(YMKH_ENOMEM, "cudaMalloc second state buffer (%zu bytes)", 24 * c->N * sizeof(double));
+  }
+  for (int i = 0; i < 12; ++i) c->buf[1].f[i] = c->own + (size_t)i * c->N;
+  for (int i = 0; i < 6; ++i) {
+    c->buf[1].a[i] = c->own + (size_t)(12 + i) * c->N;
+    c->buf[1].b[i] = c->own + (size_t)(18 + i) * c->N;
+  }
+  c->dual = false;
+  c->cur = 0;
+  c->bound = true;
+  return 0;
+}
+
+// Zero-copy form: the caller provides both buffers; after ymkh_step the
+// current state is in buffer ymkh_current_buffer().
+int ymkh_bind_state2(ymkh_ctx* c, double* const* state0, double* const* state1) {
+  if (!c || !state0 || !state1) return set_err(YMKH_EINVAL, "null argument");
+  State s0 = make_state(state0, state0 + 12, state0 + 18);
+  State s1 = make_state(state1, state1 + 12, state1 + 18);
+  if (!state_ok(s0) || !state_ok(s1)) return set_err(YMKH_EINVAL, "null state array");
+  drop_graphs(c);
+  if (c->own) { cudaFree(c->own); c->own = nullptr; }
+  c->buf[0] = s0;
+  c->buf[1] = s1;
+  c->dual = true;
+  c->cur = 0;
+  c->bound = true;
+  return 0;
+}
+
+int ymkh_current_buffer(ymkh_ctx* c) { return c ? c->cur : -1; }
+
+int ymkh_set_current_buffer(ymkh_ctx* c, int which) {
+  if (!c || (which != 0 && which != 1)) return set_err(YMKH_EINVAL, "bad buffer index");
+  if (!c->dual && which == 1) return set_err(YMKH_ESTATE, "buffer 1 is library-owned");
+  c->cur = which;
+  return 0;
+}
+
+int ymkh_init(ymkh_ctx* c, const ymkh_init_params* ip, void* stream) {
+  if (!c || !ip) return set_err(YMKH_EINVAL, "null argument");
+  if (!c->bound) return set_err(YMKH_ESTATE, "state not bound");
+  cudaStream_t s = (cudaStream_t)stream;
+  InitArgs a{};
+  a.nx = c->nx; a.nz = c->nz; a.dx = c->prm.dx; a.dz = c->prm.dz;
+  a.k_mode = ip->k_mode; a.perturb_amp = ip->perturb_amp; a.V0 = ip->V0; a.epsilon = ip->epsilon;
+  a.run_mode = ip->run_mode; a.alpha_YM = (double)(float)ip->alpha_YM;
+  a.init_by1_eq = ip->init_by1_eq; a.vz_edge_taper = ip->vz_edge_taper;
+  const double* hs[6] = {ip->seed_by, ip->seed_ex, ip->seed_ez, ip->seed_az, ip->seed_qA, ip->seed_qB};
+  const double** ds[6] = {&a.by, &a.ex, &a.ez, &a.az, &a.qA, &a.qB};
+  double* seedbuf = nullptr;
+  int nseed = 0;
+  for (int k = 0; k < 6; ++k) if (hs[k]) ++nseed;
+  if (nseed) {
+    CK(cudaMalloc(&seedbuf, (size_t)6 * c->nx * sizeof(double)), "cudaMalloc seed");
+    for (int k = 0; k < 6; ++k) {
+      if (!hs[k]) continue;
+      double* d = seedbuf + (size_t)k * c->nx;
+      CK(cudaMemcpyAsync(d, hs[k], c->nx * sizeof(double), cudaMemcpyHostToDevice, s), "seed upload");
+      *ds[k] = d;
+    }
+  }
+  c->cur = 0;
+  cudaError_t e = launch_init(c->buf[0], a, s);
+  g_launches++;
+  if (seedbuf) {
+    cudaStreamSynchronize(s);
+    cudaFree(seedbuf);
+  }
+  CK(e, "init kernel");
+  return 0;
+}
+
+int ymkh_step(ymkh_ctx* c, int nsteps, void* stream) {
+  if (!c) return set_err(YMKH_EINVAL, "null context");
+  if (!c->bound) return set_err(YMKH_ESTATE, "state not bound");
+  if (nsteps < 0) return set_err(YMKH_EINVAL, "negative step count");
+  cudaStream_t s = (cudaStream_t)stream;
+  int done = 0;
+  const bool graphs = s != nullptr && c->graph_steps >= 2 && (c->graph_steps % 2) == 0;
+  if (graphs) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cs);
+    if (cs == cudaStreamCaptureStatusNone) {
+      while (nsteps - done >= c->graph_steps) {
+        int rc = run_graph(c, s);
+        if (rc) return rc;
+        done += c->graph_steps;
+      }
+    }
+  }
+  for (; done < nsteps; ++done) {
+    int rc = step_once(c, s);
+    if (rc) return rc;
+  }
+  if (!c->dual && c->cur == 1) return copy_back(c, s);
+  return 0;
+}
+
+int ymkh_set_graph_steps(ymkh_ctx* c, int n) {
+  if (!c || n < 0 || (n % 2) != 0) return set_err(YMKH_EINVAL, "graph step count must be even and >= 0");
+  drop_graphs(c);
+  c->graph_steps = n;
+  return 0;
+}
+
+int ymkh_set_fct_shape(ymkh_ctx* c, int tx, int seg) {
+  if (!c || (tx != 32 && tx != 64 && tx != 128) || seg < 1) return set_err(YMKH_EINVAL, "bad FCT launch shape");
+  drop_graphs(c);
+  CK(prepare_fct(tx), "FCT kernel attributes");
+  c->fct_tx = tx;
+  c->fct_seg = seg;
+  return 0;
+}
+
+int ymkh_get_fct_shape(ymkh_ctx* c, int* tx, int* seg) {
+  if (!c) return set_err(YMKH_EINVAL, "null context");
+  if (tx) *tx = c->fct_tx;
+  if (seg) *seg = c->fct_seg;
+  return 0;
+}
+
+// Runs nsteps plain (uncaptured) steps with an event between stages and
+// accumulates the device time of each stage into out_ms[0..ST_COUNT).
+int ymkh_stage_times(ymkh_ctx* c, int nsteps, void* stream, float* out_ms, int nout) {
+  if (!c || !out_ms || nout < ST_COUNT) return set_err(YMKH_EINVAL, "bad arguments");
+  if (!c->bound) return set_err(YMKH_ESTATE, "state not bound");
+  cudaStream_t s = (cudaStream_t)stream;
+  for (int i = 0; i <= ST_COUNT; ++i) CK(cudaEventCreate(&c->ev[i]), "cudaEventCreate");
+  for (int i = 0; i < ST_COUNT; ++i) out_ms[i] = 0.f;
+  c->timing = true;
+  int rc = 0;
+  for (int k = 0; k < nsteps && !rc; ++k) {
+    rc = step_once(c, s);
+    if (rc) break;
+    cudaError_t e = cudaEventSynchronize(c->ev[ST_COUNT]);
+    if (e != cudaSuccess) { rc = set_err(YMKH_ECUDA, "stage timing: %s", cudaGetErrorString(e)); break; }
+    for (int i = 0; i < ST_COUNT; ++i) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, c->ev[i], c->ev[i + 1]);
+      out_ms[i] += ms;
+    }
+  }
+  c->timing = false;
+  for (int i = 0; i <= ST_COUNT; ++i) cudaEventDestroy(c->ev[i]);
+  if (!rc && !c->dual && c->cur == 1) rc = copy_back(c, s);
+  return rc;
+}
+
+int ymkh_energy_async(ymkh_ctx* c, double* dev_out, void* stream) {
+  if (!c || !dev_out) return set_err(YMKH_EINVAL, "null argument");
+  if (!c->bound) return set_err(YMKH_ESTATE, "state not bound");
+  CK(launch_energy(c->buf[c->cur], c->N, c->epart, dev_out, (cudaStream_t)stream), "energy kernels");
+  g_launches += 2;
+  return 0;
+}
+
+int ymkh_energy(ymkh_ctx* c, double* host_out, void* stream) {
+  if (!host_out) return set_err(YMKH_EINVAL, "null argument");
+  int rc = ymkh_energy_async(c, c ? c->edev : nullptr, stream);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(host_out, c->edev, sizeof(double), cudaMemcpyDeviceToHost, (cudaStream_t)stream), "energy D2H");
+  CK(cudaStreamSynchronize((cudaStream_t)stream), "energy sync");
+  return 0;
+}
+
+int ymkh_mode_amp(ymkh_ctx* c, int k, double* host_out2, void* stream) {
+  if (!c || !host_out2) return set_err(YMKH_EINVAL, "null argument");
+  if (!c->bound) return set_err(YMKH_ESTATE, "state not bound");
+  cudaStream_t s = (cudaStream_t)stream;
+  const State& st = c->buf[c->cur];
+  CK(launch_mode_amp(st.f[AZ2], st.f[AZ3], c->nx, c->nz, k, c->mcol, c->edev + 1, s), "mode amplitude kernels");
+  g_launches += 2;
+  CK(cudaMemcpyAsync(host_out2, c->edev + 1, 2 * sizeof(double), cudaMemcpyDeviceToHost, s), "mode amp D2H");
+  CK(cudaStreamSynchronize(s), "mode amp sync");
+  return 0;
+}
+
+int ymkh_destroy(ymkh_ctx* c) {
+  if (!c) return 0;
+  drop_graphs(c);
+  free_bands(c);
+  if (c->own) cudaFree(c->own);
+  if (c->epart) cudaFree(c->epart);
+  if (c->edev) cudaFree(c->edev);
+  if (c->mcol) cudaFree(c->mcol);
+  delete c;
+  return 0;
+}
+
+int ymkh_twiddles(int nz, int m_lo, int m_hi, float* cos_out, float* sin_out) {
+  if (nz < 1 || m_lo < 0 || m_hi < m_lo || !cos_out || !sin_out) return set_err(YMKH_EINVAL, "bad arguments");
+  const size_t n = (size_t)(m_hi - m_lo + 1) * nz;
+  float *dc = nullptr, *ds = nullptr;
+  CK(cudaMalloc(&dc, n * sizeof(float)), "cudaMalloc");
+  CK(cudaMalloc(&ds, n * sizeof(float)), "cudaMalloc");
+  cudaError_t e = launch_twiddles_f32(dc, ds, nz, m_lo, m_hi, 0);
+  g_launches++;
+  if (e == cudaSuccess) e = cudaMemcpy(cos_out, dc, n * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(sin_out, ds, n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(dc);
+  cudaFree(ds);
+  CK(e, "twiddle table");
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,411 @@
+// ymkh_column.cu — post-Maxwell stages that act along z or pointwise:
+// sponge (YM_Physics.cu:161-182), xi_cut (:192-210), z-mean removal
+// (:272-327), the DFT kz band filters (:349-584), z-hyperdiffusion (:228-259)
+// and the colour-1 zeroing (ymgpu2d/main_ym.cu:443-447).  All update the new
+// state buffer in place; none reads a neighbour another CTA writes.
+//
+// The band filter is written as two dense FP64 contractions per band, over
+// all filtered arrays at once (21 arrays: the 15 EM/colour arrays of
+// YM_Physics.cu:373-379 and n, px, pz of both beams):
+//   C[j, x] = inv2 * sum_z W[z, j] G[z, x]          (coefficients A_m, B_m)
+//   G[z, x] = G[z, x] - sum_j W[z, j] C[j, x]       (subtract the band)
+// with W[z, 2i] = cosf(phase), W[z, 2i+1] = sinf(phase) the reference's FP32
+// twiddles (YM_Physics.cu:387-388) widened to double and inv2 = 2.0f/nz
+// (:425).  Summation order differs from the reference's warp-shuffle tree;
+// the result agrees to rounding.
+
+#include "ymkh_common.cuh"
+
+namespace ymkh {
+
+// ---------------------------------------------------------------- twiddles
+// W[z * ldw + 2*(m-lo) + {0,1}] for m in [lo, hi].
+__global__ void twiddle_kernel(double* W, int nz, int lo, int hi, int ldw) {
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int m = lo + blockIdx.y;
+  if (z >= nz || m > hi) return;
+  float phase = 2.0f * (float)M_PI * m * z / (float)nz;
+  float cz = cosf(phase), sz = sinf(phase);
+  W[(size_t)z * ldw + 2 * (m - lo)] = (double)cz;
+  W[(size_t)z * ldw + 2 * (m - lo) + 1] = (double)sz;
+}
+
+__global__ void twiddle_f32_kernel(float* c, float* s, int nz, int lo, int hi) {
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int m = lo + blockIdx.y;
+  if (z >= nz || m > hi) return;
+  float phase = 2.0f * (float)M_PI * m * z / (float)nz;
+  c[(size_t)(m - lo) * nz + z] = cosf(phase);
+  s[(size_t)(m - lo) * nz + z] = sinf(phase);
+}
+
+cudaError_t launch_twiddles(double* W, int nz, int lo, int hi, int ldw, cudaStream_t s) {
+  dim3 grid((nz + 127) / 128, hi - lo + 1);
+  twiddle_kernel<<<grid, 128, 0, s>>>(W, nz, lo, hi, ldw);
+  return cudaGetLastError();
+}
+cudaError_t launch_twiddles_f32(float* c, float* sn, int nz, int lo, int hi, cudaStream_t s) {
+  dim3 grid((nz + 127) / 128, hi - lo + 1);
+  twiddle_f32_kernel<<<grid, 128, 0, s>>>(c, sn, nz, lo, hi);
+  return cudaGetLastError();
+}
+
+
+// ---------------------------------------------------------- sponge / xicut
+__global__ void sponge_xicut_kernel(const __grid_constant__ ArrayList a12, StepParams p, int cut) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int z = blockIdx.y;
+  if (x >= p.nx) return;
+  const double xc = (p.nx * p.dx) * 0.5;
+  const double xi = fabs((x * p.dx - xc) / p.epsilon);
+  const size_t i = idx2(x, z, p.nx);
+  if (cut) {
+    if (xi <= p.xi_cut) return;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) a12.p[k][i] = 0.0;
+  } else {
+    if (xi <= p.xi_sponge) return;
+    const double sig = p.sigma_sponge * (xi - p.xi_sponge);
+    const double dec = exp(-sig * p.dt);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) a12.p[k][i] *= dec;
+  }
+}
+
+cudaError_t launch_sponge_xicut(const ArrayList& a12, const StepParams& p, int cut, cudaStream_t s) {
+  dim3 grid((p.nx + 127) / 128, p.nz);
+  sponge_xicut_kernel<<<grid, 128, 0, s>>>(a12, p, cut);
+  return cudaGetLastError();
+}
+
+// -------------------------------------------------------------- z-mean
+// One CTA per (4 columns, array).  The column sum uses the reference's
+// halving tree (YM_Physics.cu:301-308) so the mean is bit-identical.
+constexpr int ZM_CX = 4;
+__global__ void zmean_kernel(const __grid_constant__ ArrayList a15, int nx, int nz) {
+  extern __shared__ double sm[];  // [nz][ZM_CX]
+  const int x0 = blockIdx.x * ZM_CX;
+  double* g = a15.p[blockIdx.y];
+  for (int i = threadIdx.x; i < nz * ZM_CX; i += blockDim.x) {
+    const int z = i / ZM_CX, c = i - z * ZM_CX;
+    sm[i] = (x0 + c < nx) ? g[idx2(x0 + c, z, nx)] : 0.0;
+  }
+  __syncthreads();
+  for (int st = nz >> 1; st > 0; st >>= 1) {
+    for (int i = threadIdx.x; i < st * ZM_CX; i += blockDim.x) sm[i] += sm[i + st * ZM_CX];
+    __syncthreads();
+  }
+  const double inv = 1.0 / (double)nz;
+  for (int i = threadIdx.x; i < nz * ZM_CX; i += blockDim.x) {
+    const int z = i / ZM_CX, c = i - z * ZM_CX;
+    if (x0 + c < nx) {
+      const size_t gi = idx2(x0 + c, z, nx);
+      g[gi] -= sm[c] * inv;
+    }
+  }
+}
+
+cudaError_t launch_zmean(const ArrayList& a15, int nx, int nz, cudaStream_t s) {
+  const size_t smem = (size_t)nz * ZM_CX * sizeof(double);
+  dim3 grid((nx + ZM_CX - 1) / ZM_CX, 15);
+  zmean_kernel<<<grid, 256, smem, s>>>(a15, nx, nz);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------- hyperdiffusion
+// Race-free form of YM_Physics.cu:228-259: every stencil reads the values
+// from before the update (the reference's in-place version reads a mix).
+constexpr int HD_CX = 4;
+__global__ void hyperdiff_kernel(const __grid_constant__ ArrayList a12, int nx, int nz, double mu) {
+  extern __shared__ double sm[];  // [nz][HD_CX]
+  const int x0 = blockIdx.x * HD_CX;
+  double* g = a12.p[blockIdx.y];
+  for (int i = threadIdx.x; i < nz * HD_CX; i += blockDim.x) {
+    const int z = i / HD_CX, c = i - z * HD_CX;
+    sm[i] = (x0 + c < nx) ? g[idx2(x0 + c, z, nx)] : 0.0;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nz * HD_CX; i += blockDim.x) {
+    const int z = i / HD_CX, c = i - z * HD_CX;
+    if (x0 + c >= nx) continue;
+    const int zm1 = (z == 0) ? nz - 1 : z - 1;
+    const int zm2 = (z <= 1) ? z - 2 + nz : z - 2;
+    const int zp1 = (z == nz - 1) ? 0 : z + 1;
+    const int zp2 = (z >= nz - 2) ? z + 2 - nz : z + 2;
+    const double d4 = sm[zm2 * HD_CX + c] - 4.0 * sm[zm1 * HD_CX + c] + 6.0 * sm[i] - 4.0 * sm[zp1 * HD_CX + c] +
+                      sm[zp2 * HD_CX + c];
+    g[idx2(x0 + c, z, nx)] = sm[i] - mu * d4;
+  }
+}
+
+cudaError_t launch_hyperdiff(const ArrayList& a12, int nx, int nz, double mu, cudaStream_t s) {
+  const size_t smem = (size_t)nz * HD_CX * sizeof(double);
+  dim3 grid((nx + HD_CX - 1) / HD_CX, 12);
+  hyperdiff_kernel<<<grid, 256, smem, s>>>(a12, nx, nz, mu);
+  return cudaGetLastError();
+}
+
+// Column kernels keep a block of whole columns in shared memory.
+cudaError_t prepare_column(int nz) {
+  const size_t smem = (size_t)nz * (ZM_CX > HD_CX ? ZM_CX : HD_CX) * sizeof(double);
+  if (smem > 200 * 1024) return cudaErrorInvalidValue;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(zmean_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(hyperdiff_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// ------------------------------------------------------------- band GEMMs
+// Register-blocked FP64 contractions, 64x64 output tiles, 256 threads with a
+// 4x4 micro-tile each, K staged through shared memory 16 at a time.
+constexpr int GB = 64, GK = 16;
+
+// C_k[j, x] = inv2 * sum_z W[z, j] * G_k[z, x];  j in [0, J), W row stride ldw.
+__global__ void __launch_bounds__(256)
+    band_coef_kernel(const __grid_constant__ ArrayList arrs, const double* __restrict__ W, int ldw, int J,
+                     double* __restrict__ C, int nx, int nz, double inv2) {
+  __shared__ double sW[GK][GB + 1];
+  __shared__ double sG[GK][GB + 1];
+  const int j0 = blockIdx.x * GB, x0 = blockIdx.y * GB, k = blockIdx.z;
+  const double* G = arrs.p[k];
+  double* Ck = C + (size_t)k * J * nx;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;  // ty -> j, tx -> x
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int z0 = 0; z0 < nz; z0 += GK) {
+    for (int i = threadIdx.x; i < GK * GB; i += 256) {
+      const int zz = i / GB, c = i - zz * GB;
+      const int z = z0 + zz;
+      sW[zz][c] = (z < nz && j0 + c < J) ? W[(size_t)z * ldw + j0 + c] : 0.0;
+      sG[zz][c] = (z < nz && x0 + c < nx) ? G[idx2(x0 + c, z, nx)] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int zz = 0; zz < GK; ++zz) {
+      double w[4], gv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) w[a] = sW[zz][ty + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) gv[b] = sG[zz][tx + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(w[a], gv[b], acc[a][b]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int j = j0 + ty + 16 * a, x = x0 + tx + 16 * b;
+      if (j < J && x < nx) Ck[(size_t)j * nx + x] = acc[a][b] * inv2;
+    }
+}
+
+// G_k[z, x] -= sum_j W[z, j] * C_k[j, x]
+__global__ void __launch_bounds__(256)
+    band_apply_kernel(const __grid_constant__ ArrayList arrs, const double* __restrict__ W, int ldw, int J,
+                      const double* __restrict__ C, int nx, int nz) {
+  __shared__ double sW[GK][GB + 1];  // [j][z]
+  __shared__ double sC[GK][GB + 1];  // [j][x]
+  const int z0 = blockIdx.x * GB, x0 = blockIdx.y * GB, k = blockIdx.z;
+  double* G = arrs.p[k];
+  const double* Ck = C + (size_t)k * J * nx;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;  // ty -> z, tx -> x
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int jb = 0; jb < J; jb += GK) {
+    for (int i = threadIdx.x; i < GK * GB; i += 256) {
+      const int jj = i / GB, c = i - jj * GB;
+      const int j = jb + jj;
+      sW[jj][c] = (j < J && z0 + c < nz) ? W[(size_t)(z0 + c) * ldw + j] : 0.0;
+      sC[jj][c] = (j < J && x0 + c < nx) ? Ck[(size_t)j * nx + x0 + c] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int jj = 0; jj < GK; ++jj) {
+      double w[4], cv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) w[a] = sW[jj][ty + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) cv[b] = sC[jj][tx + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(w[a], cv[b], acc[a][b]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int z = z0 + ty + 16 * a, x = x0 + tx + 16 * b;
+      if (z < nz && x < nx) {
+        const size_t gi = idx2(x, z, nx);
+        G[gi] = G[gi] - acc[a][b];
+      }
+    }
+}
+
+cudaError_t launch_band(const ArrayList& arrs, int narr, const double* W, int ldw, int J, double* C, int nx, int nz,
+                        double inv2, cudaStream_t s) {
+  dim3 g1((J + GB - 1) / GB, (nx + GB - 1) / GB, narr);
+  band_coef_kernel<<<g1, 256, 0, s>>>(arrs, W, ldw, J, C, nx, nz, inv2);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  dim3 g2((nz + GB - 1) / GB, (nx + GB - 1) / GB, narr);
+  band_apply_kernel<<<g2, 256, 0, s>>>(arrs, W, ldw, J, C, nx, nz);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- energy
+// Per-cell energy of YM_Energy.cu:3-21, summed with Neumaier compensation in
+// a fixed order: each CTA reduces a contiguous block of cells, a second
+// single-CTA pass reduces the CTA partials in index order.
+__device__ __forceinline__ void neumaier_add(double& s, double& c, double v) {
+  const double t = s + v;
+  if (fabs(s) >= fabs(v))
+    c += (s - t) + v;
+  else
+    c += (v - t) + s;
+  s = t;
+}
+
+constexpr int EN_THREADS = 256;
+constexpr int EN_PER_THREAD = 16;
+
+__global__ void __launch_bounds__(EN_THREADS)
+    energy_partial_kernel(const __grid_constant__ State st, size_t N, double* __restrict__ part) {
+  const size_t base = (size_t)blockIdx.x * EN_THREADS * EN_PER_THREAD;
+  double s = 0.0, c = 0.0;
+  for (int k = 0; k < EN_PER_THREAD; ++k) {
+    const size_t i = base + (size_t)k * EN_THREADS + threadIdx.x;
+    if (i >= N) break;
+    const double nA = fmax(st.a[FN][i], 1e-10);
+    const double nB = fmax(st.b[FN][i], 1e-10);
+    const double pxA = st.a[FPX][i], pzA = st.a[FPZ][i], pxB = st.b[FPX][i], pzB = st.b[FPZ][i];
+    const double keA = 0.5 * (pxA * pxA + pzA * pzA) / nA;
+    const double keB = 0.5 * (pxB * pxB + pzB * pzB) / nB;
+    double em2 = 0.0;
+    em2 = st.f[EX1][i] * st.f[EX1][i];
+    em2 = em2 + st.f[EX2][i] * st.f[EX2][i];
+    em2 = em2 + st.f[EX3][i] * st.f[EX3][i];
+    em2 = em2 + st.f[EZ1][i] * st.f[EZ1][i];
+    em2 = em2 + st.f[EZ2][i] * st.f[EZ2][i];
+    em2 = em2 + st.f[EZ3][i] * st.f[EZ3][i];
+    em2 = em2 + st.f[BY1][i] * st.f[BY1][i];
+    em2 = em2 + st.f[BY2][i] * st.f[BY2][i];
+    em2 = em2 + st.f[BY3][i] * st.f[BY3][i];
+    const double e = keA + keB + 0.5 * em2;
+    neumaier_add(s, c, e);
+  }
+  __shared__ double ss[EN_THREADS], sc[EN_THREADS];
+  ss[threadIdx.x] = s;
+  sc[threadIdx.x] = c;
+  __syncthreads();
+  for (int w = EN_THREADS / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      double a = ss[threadIdx.x], ca = sc[threadIdx.x] + sc[threadIdx.x + w];
+      neumaier_add(a, ca, ss[threadIdx.x + w]);
+      ss[threadIdx.x] = a;
+      sc[threadIdx.x] = ca;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = ss[0];
+    part[2 * blockIdx.x + 1] = sc[0];
+  }
+}
+
+__global__ void energy_final_kernel(const double* __restrict__ part, int nparts, double* out) {
+  __shared__ double ss[256], sc[256];
+  double s = 0.0, c = 0.0;
+  // thread t reduces a contiguous slice of the partials, in order
+  const int per = (nparts + 255) / 256;
+  for (int k = 0; k < per; ++k) {
+    const int i = threadIdx.x * per + k;
+    if (i >= nparts) break;
+    c += part[2 * i + 1];
+    neumaier_add(s, c, part[2 * i]);
+  }
+  ss[threadIdx.x] = s;
+  sc[threadIdx.x] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, ca = 0.0;
+    for (int t = 0; t < 256; ++t) {
+      ca += sc[t];
+      neumaier_add(a, ca, ss[t]);
+    }
+    *out = a + ca;
+  }
+}
+
+int energy_nparts(size_t N) { return (int)((N + EN_THREADS * EN_PER_THREAD - 1) / (EN_THREADS * EN_PER_THREAD)); }
+
+cudaError_t launch_energy(const State& st, size_t N, double* part, double* out, cudaStream_t s) {
+  const int np = energy_nparts(N);
+  energy_partial_kernel<<<np, EN_THREADS, 0, s>>>(st, N, part);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  energy_final_kernel<<<1, 256, 0, s>>>(part, np, out);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ mode amplitude
+// ymgpu2d/analysis/remote_timeseries.py:62-77: per column x,
+// F = sum_z (Az2 + i Az3) e^{-2 pi i k z/nz}, Fc for Az2 - i Az3;
+// out = (mean_x |F| / nz, mean_x |Fc| / nz).
+__global__ void mode_amp_kernel(const double* __restrict__ az2, const double* __restrict__ az3, int nx, int nz,
+                                int k, double* __restrict__ colbuf) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= nx) return;
+  double fr = 0, fi = 0, cr = 0, ci = 0;
+  for (int z = 0; z < nz; ++z) {
+    double sn, cs;
+    sincospi(-2.0 * (double)k * (double)z / (double)nz, &sn, &cs);
+    const double a = az2[idx2(x, z, nx)], b = az3[idx2(x, z, nx)];
+    // (a + i b)(cs + i sn)
+    fr += a * cs - b * sn;
+    fi += a * sn + b * cs;
+    // (a - i b)(cs + i sn)
+    cr += a * cs + b * sn;
+    ci += a * sn - b * cs;
+  }
+  colbuf[2 * x] = hypot(fr, fi);
+  colbuf[2 * x + 1] = hypot(cr, ci);
+}
+
+__global__ void mode_amp_final_kernel(const double* __restrict__ colbuf, int nx, int nz, double* out) {
+  if (threadIdx.x != 0) return;
+  double s0 = 0, s1 = 0;
+  for (int x = 0; x < nx; ++x) {
+    s0 += colbuf[2 * x];
+    s1 += colbuf[2 * x + 1];
+  }
+  out[0] = s0 / nx / nz;
+  out[1] = s1 / nx / nz;
+}
+
+cudaError_t launch_mode_amp(const double* az2, const double* az3, int nx, int nz, int k, double* colbuf, double* out,
+                            cudaStream_t s) {
+  mode_amp_kernel<<<(nx + 127) / 128, 128, 0, s>>>(az2, az3, nx, nz, k, colbuf);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  mode_amp_final_kernel<<<1, 32, 0, s>>>(colbuf, nx, nz, out);
+  return cudaGetLastError();
+}
+
+}  // namespace ymkh

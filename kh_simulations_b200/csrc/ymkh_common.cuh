@@ -1,0 +1,128 @@
+// ymkh_common.cuh — device helpers shared by the ymkh kernels.
+//
+// Arithmetic is written operand for operand as in the reference so that,
+// compiled with -fmad=false, results are bit-identical to the reference
+// kernels built the same way (and to the -ffp-contract=off CPU oracle).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "../../include/ymkh.h"
+
+namespace ymkh {
+
+// State order of include/ymkh.h.
+enum Field { EX1 = 0, EX2, EX3, EZ1, EZ2, EZ3, BY1, BY2, BY3, AZ1, AZ2, AZ3 };
+enum Fluid { FN = 0, FPX, FPZ, FQ1, FQ2, FQ3 };
+
+struct State {
+  double* f[YMKH_NFIELDS];
+  double* a[YMKH_NFLUID];
+  double* b[YMKH_NFLUID];
+};
+
+struct StepParams {
+  int nx, nz;
+  double dx, dz, dt, c2, eps0, alpha;
+  int freeze_az1, periodic_x;
+  double epsilon, xi_sponge, sigma_sponge, xi_cut, warm_T;
+  int suppress_kz0;
+  double hyp_diff;
+};
+
+__host__ __device__ __forceinline__ size_t idx2(int x, int z, int nx) {
+  return (size_t)x + (size_t)z * (size_t)nx;
+}
+
+// FCT_DeviceMath.cuh:38-46 (compute_eps)
+__device__ __forceinline__ double fct_eps(double uL, double uR, double dtdx) {
+  double v = 0.5 * (uL + uR);
+  return v * dtdx;
+}
+// FCT_DeviceMath.cuh:52-63 (compute_nu_mu)
+__device__ __forceinline__ void fct_nu_mu(double eps, double& nu, double& mu) {
+  double scrh = fmin(1.0 / 6.0, fabs(eps));
+  scrh = (1.0 / 3.0) * scrh * scrh;
+  nu = (1.0 / 6.0) + (1.0 / 3.0) * (eps * eps - scrh * scrh);
+  mu = 0.25 - 0.5 * nu;
+}
+// FCT_DeviceMath.cuh:108-125 (apply_fct_limiter)
+__device__ __forceinline__ double fct_limit(double f, double dm1, double d0, double dp1) {
+  double s = copysign(1.0, d0);
+  double term = s * dm1, terp = s * dp1, fa = fabs(f);
+  return s * fmax(0.0, fmin(term, fmin(fa, terp)));
+}
+
+// Periodic / clamped index maps of the shear axis (ymgpu2d/YM_FCT.cu:7-18 pad,
+// FCT_Sweeps.cu:68-81 clamped halo loads).
+__device__ __forceinline__ int xmap(int x, int nx, int periodic) {
+  if (periodic) {
+    x %= nx;
+    return x < 0 ? x + nx : x;
+  }
+  return x < 0 ? 0 : (x >= nx ? nx - 1 : x);
+}
+__device__ __forceinline__ int zclamp(int z, int nz) { return z < 0 ? 0 : (z >= nz ? nz - 1 : z); }
+__device__ __forceinline__ int zwrap(int z, int nz) {
+  z %= nz;
+  return z < 0 ? z + nz : z;
+}
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+}  // namespace ymkh
+
+namespace ymkh {
+
+// Up to 24 array pointers passed by value to the column kernels.
+struct ArrayList {
+  double* p[24];
+};
+
+// Arguments of the initial-state kernel (ymgpu2d/YM_Init.cu:32-40).
+struct InitArgs {
+  int nx, nz;
+  double dx, dz;
+  int k_mode;
+  double perturb_amp, V0, epsilon;
+  int run_mode;
+  double alpha_YM;
+  int init_by1_eq;
+  double vz_edge_taper;
+  const double* by;
+  const double* ex;
+  const double* ez;
+  const double* az;
+  const double* qA;
+  const double* qB;
+};
+
+// Launchers (one per kernel family).  prepare_* set function attributes
+// outside any stream capture.
+cudaError_t prepare_fct(int tx);
+cudaError_t launch_fct(const State& in, const State& out, const StepParams& p, int tx, int seg_len, cudaStream_t s);
+cudaError_t launch_maxwell(const State& fluid_new, const State& fields_old, const State& out, const StepParams& p,
+                           cudaStream_t s);
+cudaError_t launch_sponge_xicut(const ArrayList& a12, const StepParams& p, int cut, cudaStream_t s);
+cudaError_t prepare_column(int nz);
+cudaError_t launch_zmean(const ArrayList& a15, int nx, int nz, cudaStream_t s);
+cudaError_t launch_hyperdiff(const ArrayList& a12, int nx, int nz, double mu, cudaStream_t s);
+cudaError_t launch_band(const ArrayList& arrs, int narr, const double* W, int ldw, int J, double* C, int nx, int nz,
+                        double inv2, cudaStream_t s);
+cudaError_t launch_twiddles(double* W, int nz, int lo, int hi, int ldw, cudaStream_t s);
+cudaError_t launch_twiddles_f32(float* c, float* sn, int nz, int lo, int hi, cudaStream_t s);
+cudaError_t launch_energy(const State& st, size_t N, double* part, double* out, cudaStream_t s);
+int energy_nparts(size_t N);
+cudaError_t launch_mode_amp(const double* az2, const double* az3, int nx, int nz, int k, double* colbuf, double* out,
+                            cudaStream_t s);
+cudaError_t launch_init(const State& st, const InitArgs& a, cudaStream_t s);
+
+}  // namespace ymkh

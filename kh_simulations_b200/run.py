@@ -1,0 +1,212 @@
+"""``KHRun``: one Kelvin–Helmholtz run with its state resident in HBM.
+
+Replaces the driver ymgpu2d/main_ym.cu: configuration and derivation
+(:24-83), allocation (:85-121, here two 24-array FP64 buffers held as torch
+tensors), seed profile upload (:178-217), initial state (:219-237), the
+step loop with the energy check and halt rules (:318-479) and
+``energy.csv`` in the reference's format (:251-256, :458-466).
+The arithmetic runs in the CUDA library (include/ymkh.h); this module only
+owns memory, streams and files.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import NSTATE, STATE_NAMES, Grid, InitParams, check
+from .config import Derived, RunConfig, derive, load_config, step_params
+from .seed import load_profiles
+
+
+def init_params(cfg: RunConfig, d: Derived, profiles: dict | None = None):
+    """ymkh_init_params for the run (arguments of kernel_ym_init at
+    ymgpu2d/main_ym.cu:223-225).  Returns (params, arrays to keep alive)."""
+    ip = InitParams()
+    ip.run_mode, ip.k_mode = cfg.run_mode, cfg.k_mode
+    ip.perturb_amp, ip.V0, ip.epsilon = cfg.perturb_amp, d.V0, d.eps
+    ip.alpha_YM, ip.init_by1_eq, ip.vz_edge_taper = d.alpha, cfg.init_by1_eq, cfg.vz_edge_taper
+    keep = []
+    for k, v in (profiles or {}).items():
+        arr = np.ascontiguousarray(v, dtype=np.float64)
+        if arr.shape != (d.nx,):
+            raise ValueError(f"seed profile {k} has shape {arr.shape}, expected ({d.nx},)")
+        keep.append(arr)
+        setattr(ip, "seed_" + k, arr.ctypes.data)
+    return ip, keep
+
+
+def _stream_ptr(stream) -> int | None:
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    return stream.cuda_stream
+
+
+@dataclass
+class EnergyRecord:
+    step: int
+    time: float
+    energy: float
+    ratio: float
+
+
+class KHRun:
+    """One run.  ``state`` is a [24, NZ, NX] float64 CUDA tensor (include/ymkh.h order)."""
+
+    def __init__(self, cfg: RunConfig, device: int | str | torch.device = "cuda", *, graph_steps: int | None = None,
+                 fct_shape: tuple | None = None):
+        if not torch.cuda.is_available():
+            raise _lib.YMKHError("KHRun needs a CUDA device (no CPU fallback)")
+        self.cfg = cfg
+        self.d: Derived = derive(cfg)
+        self.device = torch.device(device)
+        self.lib = _lib.load()
+        nx, nz = self.d.nx, self.d.nz
+        with torch.cuda.device(self.device):
+            self.buf = [torch.zeros((NSTATE, nz, nx), dtype=torch.float64, device=self.device) for _ in range(2)]
+            grid = Grid(nx, nz, self.d.dx, self.d.dz)
+            self.params = step_params(cfg, self.d)
+            ctx = C.c_void_p()
+            check(self.lib.ymkh_create(C.byref(grid), C.byref(self.params), C.byref(ctx)), "ymkh_create")
+            self.ctx = ctx
+            p0 = (C.c_void_p * NSTATE)(*[self.buf[0][i].data_ptr() for i in range(NSTATE)])
+            p1 = (C.c_void_p * NSTATE)(*[self.buf[1][i].data_ptr() for i in range(NSTATE)])
+            check(self.lib.ymkh_bind_state2(self.ctx, p0, p1), "ymkh_bind_state2")
+            if graph_steps is not None:
+                check(self.lib.ymkh_set_graph_steps(self.ctx, graph_steps), "ymkh_set_graph_steps")
+            if fct_shape is not None:
+                check(self.lib.ymkh_set_fct_shape(self.ctx, *fct_shape), "ymkh_set_fct_shape")
+        self.step_count = 0
+        self.E0: float | None = None
+        self.history: list[EnergyRecord] = []
+        self.halted = False
+        self.halt_reason = ""
+
+    # ---------------------------------------------------------------- state
+    @property
+    def current(self) -> int:
+        return int(self.lib.ymkh_current_buffer(self.ctx))
+
+    @property
+    def state(self) -> torch.Tensor:
+        """The current state buffer (a view; valid until the next step)."""
+        return self.buf[self.current]
+
+    def field(self, name: str) -> torch.Tensor:
+        return self.state[STATE_NAMES.index(name)]
+
+    def set_state(self, st) -> None:
+        """Copy a [24, NZ, NX] array (numpy or torch) into the current buffer."""
+        t = torch.as_tensor(st, dtype=torch.float64)
+        if tuple(t.shape) != (NSTATE, self.d.nz, self.d.nx):
+            raise ValueError(f"state shape {tuple(t.shape)} != {(NSTATE, self.d.nz, self.d.nx)}")
+        check(self.lib.ymkh_set_current_buffer(self.ctx, 0), "ymkh_set_current_buffer")
+        self.buf[0].copy_(t.to(self.device))
+
+    def state_numpy(self) -> np.ndarray:
+        torch.cuda.synchronize(self.device)
+        return self.state.cpu().numpy()
+
+    # ----------------------------------------------------------------- init
+    def init(self, seed_file: str | Path | None = None, stream=None) -> None:
+        """kernel_ym_init with the run's parameters (main_ym.cu:219-226)."""
+        cfg, d = self.cfg, self.d
+        seed_file = seed_file if seed_file is not None else (cfg.seed_profile_file or None)
+        ip, keep = init_params(cfg, d, load_profiles(seed_file, d.nx) if seed_file else None)
+        with torch.cuda.device(self.device):
+            check(self.lib.ymkh_init(self.ctx, C.byref(ip), C.c_void_p(_stream_ptr(stream))), "ymkh_init")
+            torch.cuda.synchronize(self.device)
+        self.step_count = 0
+        self.history.clear()
+        self.halted = False
+        self.E0 = None
+
+    def add_noise(self, sigma: float = 1e-6, seed: int = 0, names=("Ex1", "Ex2", "Ex3", "Ez1", "Ez2", "Ez3",
+                                                                   "By1", "By2", "By3")) -> None:
+        """Optional N(0, sigma) field noise, drawn on the host from numpy's
+        default_rng(seed) in the given array order, then uploaded (so that a
+        CPU check sees the same numbers)."""
+        rng = np.random.default_rng(seed)
+        st = self.state
+        for nm in names:
+            noise = rng.normal(0.0, sigma, size=(self.d.nz, self.d.nx))
+            st[STATE_NAMES.index(nm)] += torch.from_numpy(noise).to(self.device)
+
+    # ----------------------------------------------------------------- step
+    def step(self, n: int = 1, stream=None) -> None:
+        with torch.cuda.device(self.device):
+            check(self.lib.ymkh_step(self.ctx, int(n), C.c_void_p(_stream_ptr(stream))), "ymkh_step")
+        self.step_count += n
+
+    def energy(self, stream=None) -> float:
+        out = C.c_double()
+        with torch.cuda.device(self.device):
+            check(self.lib.ymkh_energy(self.ctx, C.byref(out), C.c_void_p(_stream_ptr(stream))), "ymkh_energy")
+        return out.value
+
+    def mode_amp(self, k: int | None = None, stream=None) -> tuple:
+        out = (C.c_double * 2)()
+        k = self.cfg.k_mode if k is None else k
+        with torch.cuda.device(self.device):
+            check(self.lib.ymkh_mode_amp(self.ctx, int(k), out, C.c_void_p(_stream_ptr(stream))), "ymkh_mode_amp")
+        return out[0], out[1]
+
+    # ------------------------------------------------------------------ loop
+    def run(self, total_steps: int | None = None, energy_stride: int | None = None, csv: str | Path | None = None,
+            on_energy=None, stream=None) -> list:
+        """The time loop of ymgpu2d/main_ym.cu:318-479 (without CSV snapshots):
+        energy every ``energy_stride`` steps, halt on NaN/Inf or E/E0 above
+        the reference's threshold (:249, :467-474)."""
+        d = self.d
+        total = d.total_steps if total_steps is None else total_steps
+        stride = d.energy_stride if energy_stride is None else energy_stride
+        fh = open(csv, "w") if csv else None
+        try:
+            if self.E0 is None:
+                self.E0 = self.energy(stream)
+                self.history.append(EnergyRecord(0, 0.0, self.E0, 1.0))
+                if fh:
+                    fh.write("step,time,E_total,E_ratio\n")
+                    fh.write(f"0,0,{self.E0:.8e},1.0\n")
+            while self.step_count < total and not self.halted:
+                n = min(stride - (self.step_count % stride), total - self.step_count)
+                self.step(n, stream)
+                if self.step_count % stride == 0:
+                    E = self.energy(stream)
+                    ratio = E / self.E0
+                    t = self.step_count * d.dt
+                    rec = EnergyRecord(self.step_count, t, E, ratio)
+                    self.history.append(rec)
+                    if fh:
+                        fh.write(f"{self.step_count},{t:.8e},{E:.8e},{ratio:.8e}\n")
+                        fh.flush()
+                    if on_energy:
+                        on_energy(self, rec)
+                    if math.isnan(E) or math.isinf(E):
+                        self.halted, self.halt_reason = True, f"NaN/Inf at t={t}"
+                    elif ratio > d.energy_thresh:
+                        self.halted, self.halt_reason = True, f"E/E0={ratio} > {d.energy_thresh} at t={t}"
+        finally:
+            if fh:
+                fh.close()
+        return self.history
+
+    def close(self) -> None:
+        if getattr(self, "ctx", None):
+            self.lib.ymkh_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @classmethod
+    def from_ini(cls, path: str | Path, **kw) -> "KHRun":
+        return cls(load_config(path), **kw)

@@ -1,0 +1,342 @@
+// ref_harness.cu — drives the reference's OWN kernels (ymgpu2d/*.cu, compiled
+// unmodified from the reference tree by oracle/Makefile) through the stage
+// sequence of its time loop, ymgpu2d/main_ym.cu:322-479, and exposes it as a C
+// library for the tests and for the reference timing leg of bench.py.
+//
+// TEST INFRASTRUCTURE ONLY (see oracle/ym_oracle.cpp for the rule).
+//
+// Differences from main_ym.cu, all outside the arithmetic:
+//  - no output directory, CSV snapshots or energy.csv; state is exchanged as
+//    raw FP64 host arrays in the include/ymkh.h order;
+//  - every launch is checked (the reference checks none);
+//  - optional raise of the dynamic shared-memory limit of
+//    kernel_ym_subtract_zmean so that NZ = 512 / 1024 run as intended (the
+//    stock loop silently skips that kernel there: 15*NZ*8 B > 48 KB);
+//  - the extension bands of ymkh_params are applied with the reference's own
+//    band kernels, after its two standard bands.
+// The call order of main_ym.cu is kept exactly, including the D2D copies.
+
+#include <cstdio>
+#include <cstring>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "YM_Fluid.cuh"
+#include "YM_Init.cuh"
+#include "YM_Energy.cuh"
+#include "YM_FCT.cuh"
+
+#include "../include/ymkh.h"
+
+namespace {
+
+struct Ref {
+  int nx = 0, nz = 0, np = 0;
+  size_t bytes = 0;
+  GridParams grid{};
+  YMParams params{};
+  ymkh_params kp{};
+  bool raise_smem = false;
+  YMFieldPtrs f{};
+  YMFluidPtrs flA{}, flA_old{}, srcA{}, flA_t{}, flA_old_t{}, srcA_t{};
+  YMFluidPtrs flB{}, flB_old{}, srcB{}, flB_t{}, flB_old_t{}, srcB_t{};
+  double *sQ1A{}, *sQ2A{}, *sQ3A{}, *sQ1A_t{}, *sQ2A_t{}, *sQ3A_t{};
+  double *sQ1B{}, *sQ2B{}, *sQ3B{}, *sQ1B_t{}, *sQ2B_t{}, *sQ3B_t{};
+  double *pad_n{}, *pad_ux{}, *pad_var{}, *pad_new{}, *pad_src{}, *pad_eth{};
+  double* ebuf{};
+  std::vector<double> h_ebuf;
+  std::vector<void*> allocs;
+  bool live = false;
+};
+
+Ref g;
+char g_err[512] = "";
+
+int fail(const char* what, cudaError_t e) {
+  snprintf(g_err, sizeof g_err, "%s: %s", what, cudaGetErrorString(e));
+  return YMKH_ECUDA;
+}
+#define RCHK(call)                                   \
+  do {                                               \
+    cudaError_t e_ = (call);                         \
+    if (e_ != cudaSuccess) return fail(#call, e_);   \
+  } while (0)
+#define RLAUNCH(what)                                \
+  do {                                               \
+    cudaError_t e_ = cudaGetLastError();             \
+    if (e_ != cudaSuccess) return fail(what, e_);    \
+  } while (0)
+
+double* dalloc(size_t bytes) {
+  void* p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+  cudaMemset(p, 0, bytes);
+  g.allocs.push_back(p);
+  return (double*)p;
+}
+
+void fluid_alloc(YMFluidPtrs& fl) {
+  fl.n = dalloc(g.bytes); fl.ux = dalloc(g.bytes); fl.uy = dalloc(g.bytes);
+  fl.px = dalloc(g.bytes); fl.pz = dalloc(g.bytes);
+  fl.Q1 = dalloc(g.bytes); fl.Q2 = dalloc(g.bytes); fl.Q3 = dalloc(g.bytes);
+  fl.E_therm = dalloc(g.bytes);
+}
+
+double** state_ptr(int i) {
+  static double** t[YMKH_NSTATE];
+  double** v[YMKH_NSTATE] = {
+      &g.f.Ex1, &g.f.Ex2, &g.f.Ex3, &g.f.Ez1, &g.f.Ez2, &g.f.Ez3,
+      &g.f.By1, &g.f.By2, &g.f.By3, &g.f.Az1, &g.f.Az2, &g.f.Az3,
+      &g.flA.n, &g.flA.px, &g.flA.pz, &g.flA.Q1, &g.flA.Q2, &g.flA.Q3,
+      &g.flB.n, &g.flB.px, &g.flB.pz, &g.flB.Q1, &g.flB.Q2, &g.flB.Q3};
+  for (int k = 0; k < YMKH_NSTATE; ++k) t[k] = v[k];
+  return t[i];
+}
+
+dim3 th2() { return dim3(16, 16); }
+dim3 bl2() { return dim3((g.nx + 15) / 16, (g.nz + 15) / 16); }
+
+// ymgpu2d/main_ym.cu:228-237 (velocities and sources for the next FCT).
+int precompute() {
+  kernel_update_velocities<<<bl2(), th2()>>>(g.flA, g.nx, g.nz);
+  kernel_update_velocities<<<bl2(), th2()>>>(g.flB, g.nx, g.nz);
+  kernel_ym_lorentz<<<bl2(), th2()>>>(g.srcA, g.f, g.flA, g.nx, g.nz, g.params.periodic_x,
+                                      g.params.warm_T, g.params.dx, g.params.dz);
+  kernel_ym_lorentz<<<bl2(), th2()>>>(g.srcB, g.f, g.flB, g.nx, g.nz, g.params.periodic_x,
+                                      g.params.warm_T, g.params.dx, g.params.dz);
+  kernel_ym_precession<<<bl2(), th2()>>>(g.sQ1A, g.sQ2A, g.sQ3A, g.f, g.flA, g.params.alpha_YM, g.nx, g.nz);
+  kernel_ym_precession<<<bl2(), th2()>>>(g.sQ1B, g.sQ2B, g.sQ3B, g.f, g.flB, g.params.alpha_YM, g.nx, g.nz);
+  RLAUNCH("precompute");
+  RCHK(cudaDeviceSynchronize());
+  return 0;
+}
+
+int band_em(int lo, int hi) {
+  int nwarps = g.nz / 32;
+  size_t smem = (2 * nwarps + 2) * 15 * sizeof(double);
+  kernel_ym_subtract_kz_range<<<g.nx, g.nz, smem>>>(g.f, g.flA, g.flB, g.nx, g.nz, lo, hi);
+  RLAUNCH("kernel_ym_subtract_kz_range");
+  return 0;
+}
+
+int band_fluid(int lo, int hi) {
+  int nwarps = g.nz / 32;
+  size_t smem = (2 * nwarps + 2) * 2 * sizeof(double);
+  kernel_fluid_pz_subtract_kz_range<<<g.nx, g.nz, smem>>>(g.flA.pz, g.flB.pz, g.nx, g.nz, lo, hi);
+  kernel_fluid_pz_subtract_kz_range<<<g.nx, g.nz, smem>>>(g.flA.px, g.flB.px, g.nx, g.nz, lo, hi);
+  kernel_fluid_n_subtract_kz_range<<<g.nx, g.nz, smem>>>(g.flA.n, g.flB.n, g.nx, g.nz, lo, hi);
+  RLAUNCH("fluid band kernels");
+  return 0;
+}
+
+// One iteration of ymgpu2d/main_ym.cu:324-455.
+int step_once() {
+  const double DT = g.params.dt_step;
+  kernel_update_velocities<<<bl2(), th2()>>>(g.flA, g.nx, g.nz);
+  kernel_update_velocities<<<bl2(), th2()>>>(g.flB, g.nx, g.nz);
+  RLAUNCH("velocities");
+
+  copy_ym_fluid(g.flA_old, g.flA, g.bytes);
+  if (g.params.periodic_x)
+    ym_fct_x_sweep_periodic(g.flA_old, g.flA, g.srcA, g.sQ1A, g.sQ2A, g.sQ3A, g.grid, DT, g.np,
+                            g.pad_n, g.pad_ux, g.pad_var, g.pad_new, g.pad_src, g.pad_eth);
+  else
+    ym_fct_x_sweep(g.flA_old, g.flA, g.srcA, g.sQ1A, g.sQ2A, g.sQ3A, g.grid, DT);
+  copy_ym_fluid(g.flB_old, g.flB, g.bytes);
+  if (g.params.periodic_x)
+    ym_fct_x_sweep_periodic(g.flB_old, g.flB, g.srcB, g.sQ1B, g.sQ2B, g.sQ3B, g.grid, DT, g.np,
+                            g.pad_n, g.pad_ux, g.pad_var, g.pad_new, g.pad_src, g.pad_eth);
+  else
+    ym_fct_x_sweep(g.flB_old, g.flB, g.srcB, g.sQ1B, g.sQ2B, g.sQ3B, g.grid, DT);
+  RLAUNCH("x sweeps");
+
+  copy_ym_fluid(g.flA_old, g.flA, g.bytes);
+  ym_fct_z_sweep(g.flA_old, g.flA, g.srcA, g.sQ1A, g.sQ2A, g.sQ3A, g.flA_old_t, g.flA_t, g.srcA_t,
+                 g.sQ1A_t, g.sQ2A_t, g.sQ3A_t, g.grid, DT);
+  copy_ym_fluid(g.flB_old, g.flB, g.bytes);
+  ym_fct_z_sweep(g.flB_old, g.flB, g.srcB, g.sQ1B, g.sQ2B, g.sQ3B, g.flB_old_t, g.flB_t, g.srcB_t,
+                 g.sQ1B_t, g.sQ2B_t, g.sQ3B_t, g.grid, DT);
+  RLAUNCH("z sweeps");
+
+  kernel_enforce_boundaries<<<bl2(), th2()>>>(g.f, g.flA, g.flB, g.nx, g.nz, g.params.periodic_x);
+  kernel_ym_currents<<<bl2(), th2()>>>(g.f, g.flA, g.flB, g.nx, g.nz, g.params);
+  kernel_ym_ampere<<<bl2(), th2()>>>(g.f, g.params, g.nx, g.nz);
+  kernel_ym_potential<<<bl2(), th2()>>>(g.f, g.params, g.nx, g.nz);
+  kernel_ym_faraday<<<bl2(), th2()>>>(g.f, g.params, g.nx, g.nz);
+  RLAUNCH("maxwell");
+  if (g.params.xi_sponge > 0.0)
+    kernel_ym_sponge<<<bl2(), th2()>>>(g.f, g.flA, g.flB, g.nx, g.nz, g.params);
+  if (g.params.xi_cut > 0.0)
+    kernel_ym_xicut<<<bl2(), th2()>>>(g.f, g.flA, g.flB, g.nx, g.nz, g.params);
+  RLAUNCH("sponge/xicut");
+  if (g.params.suppress_kz0) {
+    size_t smem = 15 * g.nz * sizeof(double);
+    kernel_ym_subtract_zmean<<<g.nx, g.nz, smem>>>(g.f, g.flA, g.flB, g.nx, g.nz);
+    RLAUNCH("kernel_ym_subtract_zmean");
+  }
+  if (g.params.kz_suppress_max >= 1 && band_em(1, g.params.kz_suppress_max)) return YMKH_ECUDA;
+  if (g.params.kz_suppress_hi > g.params.kz_suppress_max + 1 &&
+      band_em(g.params.kz_suppress_max + 2, g.params.kz_suppress_hi))
+    return YMKH_ECUDA;
+  for (int b = 0; b < g.kp.n_extra_bands; ++b)
+    if (band_em(g.kp.extra_band_lo[b], g.kp.extra_band_hi[b])) return YMKH_ECUDA;
+  if (g.params.kz_suppress_max >= 1 && band_fluid(1, g.params.kz_suppress_max)) return YMKH_ECUDA;
+  if (g.params.kz_suppress_hi > g.params.kz_suppress_max + 1 &&
+      band_fluid(g.params.kz_suppress_max + 2, g.params.kz_suppress_hi))
+    return YMKH_ECUDA;
+  for (int b = 0; b < g.kp.n_extra_bands; ++b)
+    if (band_fluid(g.kp.extra_band_lo[b], g.kp.extra_band_hi[b])) return YMKH_ECUDA;
+  if (g.params.hyp_diff_coeff > 0.0f)
+    kernel_ym_hyperdiffuse_z<<<bl2(), th2()>>>(g.f, g.flA, g.flB, g.nx, g.nz, g.params.hyp_diff_coeff);
+  if (g.params.suppress_kz0) {
+    RCHK(cudaMemset(g.f.By1, 0, g.bytes));
+    RCHK(cudaMemset(g.f.Ex1, 0, g.bytes));
+    RCHK(cudaMemset(g.f.Ez1, 0, g.bytes));
+  }
+  kernel_ym_lorentz<<<bl2(), th2()>>>(g.srcA, g.f, g.flA, g.nx, g.nz, g.params.periodic_x,
+                                      g.params.warm_T, g.params.dx, g.params.dz);
+  kernel_ym_lorentz<<<bl2(), th2()>>>(g.srcB, g.f, g.flB, g.nx, g.nz, g.params.periodic_x,
+                                      g.params.warm_T, g.params.dx, g.params.dz);
+  kernel_ym_precession<<<bl2(), th2()>>>(g.sQ1A, g.sQ2A, g.sQ3A, g.f, g.flA, g.params.alpha_YM, g.nx, g.nz);
+  kernel_ym_precession<<<bl2(), th2()>>>(g.sQ1B, g.sQ2B, g.sQ3B, g.f, g.flB, g.params.alpha_YM, g.nx, g.nz);
+  RLAUNCH("sources");
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ymref_last_error(void) { return g_err; }
+
+int ymref_destroy(void) {
+  for (void* p : g.allocs) cudaFree(p);
+  g.allocs.clear();
+  g.live = false;
+  return 0;
+}
+
+// Allocation as ymgpu2d/main_ym.cu:85-121.
+int ymref_create(const ymkh_grid* grid, const ymkh_params* p, int raise_zmean_smem) {
+  if (g.live) ymref_destroy();
+  if (!grid || !p || grid->nx < 8 || grid->nz < 8) { snprintf(g_err, sizeof g_err, "bad grid"); return YMKH_EINVAL; }
+  g.nx = grid->nx; g.nz = grid->nz; g.np = g.nx + 2 * FCT_HALO;
+  g.bytes = (size_t)g.nx * g.nz * sizeof(double);
+  g.grid = GridParams{g.nx, g.nz, grid->dx, grid->dz};
+  g.kp = *p;
+  YMParams& q = g.params;
+  q.dx = p->dx; q.dz = p->dz; q.dt_step = p->dt_step; q.c = p->c; q.eps_0 = p->eps_0;
+  q.alpha_YM = p->alpha_YM; q.V0 = p->V0; q.epsilon = p->epsilon;
+  q.freeze_az1 = p->freeze_az1; q.periodic_x = p->periodic_x;
+  q.xi_sponge = p->xi_sponge; q.sigma_sponge = p->sigma_sponge; q.xi_cut = p->xi_cut;
+  q.warm_T = p->warm_T; q.suppress_kz0 = p->suppress_kz0; q.hyp_diff_coeff = p->hyp_diff_coeff;
+  q.kz_suppress_max = p->kz_suppress_max; q.kz_suppress_hi = p->kz_suppress_hi;
+  g.raise_smem = raise_zmean_smem != 0;
+
+  double** fp[18] = {&g.f.Ex1, &g.f.Ex2, &g.f.Ex3, &g.f.Ez1, &g.f.Ez2, &g.f.Ez3,
+                     &g.f.By1, &g.f.By2, &g.f.By3, &g.f.Az1, &g.f.Az2, &g.f.Az3,
+                     &g.f.Jx1, &g.f.Jx2, &g.f.Jx3, &g.f.Jz1, &g.f.Jz2, &g.f.Jz3};
+  for (auto* x : fp) *x = dalloc(g.bytes);
+  for (YMFluidPtrs* fl : {&g.flA, &g.flA_old, &g.srcA, &g.flA_t, &g.flA_old_t, &g.srcA_t,
+                          &g.flB, &g.flB_old, &g.srcB, &g.flB_t, &g.flB_old_t, &g.srcB_t})
+    fluid_alloc(*fl);
+  for (double** x : {&g.sQ1A, &g.sQ2A, &g.sQ3A, &g.sQ1A_t, &g.sQ2A_t, &g.sQ3A_t,
+                     &g.sQ1B, &g.sQ2B, &g.sQ3B, &g.sQ1B_t, &g.sQ2B_t, &g.sQ3B_t})
+    *x = dalloc(g.bytes);
+  if (q.periodic_x) {
+    size_t pb = (size_t)g.np * g.nz * sizeof(double);
+    g.pad_n = dalloc(pb); g.pad_ux = dalloc(pb); g.pad_var = dalloc(pb);
+    g.pad_new = dalloc(pb); g.pad_src = dalloc(pb); g.pad_eth = dalloc(pb);
+  }
+  g.ebuf = dalloc(g.bytes);
+  g.h_ebuf.assign((size_t)g.nx * g.nz, 0.0);
+  for (void* a : g.allocs)
+    if (!a) { snprintf(g_err, sizeof g_err, "cudaMalloc failed"); ymref_destroy(); return YMKH_ENOMEM; }
+  if (g.raise_smem) {
+    RCHK(cudaFuncSetAttribute(kernel_ym_subtract_zmean, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(15 * g.nz * sizeof(double))));
+  }
+  g.live = true;
+  RCHK(cudaDeviceSynchronize());
+  return 0;
+}
+
+// kernel_ym_init + precompute, ymgpu2d/main_ym.cu:219-237.
+int ymref_init(const ymkh_init_params* ip) {
+  if (!g.live || !ip) return YMKH_ESTATE;
+  YMSeedProfiles seed{};
+  std::vector<double*> tmp;
+  const double* hs[6] = {ip->seed_by, ip->seed_ex, ip->seed_ez, ip->seed_az, ip->seed_qA, ip->seed_qB};
+  const double** ds[6] = {&seed.by, &seed.ex, &seed.ez, &seed.az, &seed.qA, &seed.qB};
+  for (int k = 0; k < 6; ++k) {
+    if (!hs[k]) continue;
+    double* d = nullptr;
+    RCHK(cudaMalloc(&d, g.nx * sizeof(double)));
+    RCHK(cudaMemcpy(d, hs[k], g.nx * sizeof(double), cudaMemcpyHostToDevice));
+    tmp.push_back(d);
+    *ds[k] = d;
+  }
+  kernel_ym_init<<<bl2(), th2()>>>(g.f, g.flA, g.flB, g.nx, g.nz, g.params.dx, g.params.dz,
+                                   ip->k_mode, ip->perturb_amp, ip->V0, ip->epsilon, ip->run_mode,
+                                   (float)ip->alpha_YM, ip->init_by1_eq, ip->vz_edge_taper, seed);
+  RLAUNCH("kernel_ym_init");
+  RCHK(cudaDeviceSynchronize());
+  for (double* d : tmp) cudaFree(d);
+  return precompute();
+}
+
+int ymref_set_state(double* const* host24) {
+  if (!g.live) return YMKH_ESTATE;
+  for (int i = 0; i < YMKH_NSTATE; ++i)
+    RCHK(cudaMemcpy(*state_ptr(i), host24[i], g.bytes, cudaMemcpyHostToDevice));
+  return precompute();
+}
+
+int ymref_get_state(double* const* host24) {
+  if (!g.live) return YMKH_ESTATE;
+  RCHK(cudaDeviceSynchronize());
+  for (int i = 0; i < YMKH_NSTATE; ++i)
+    RCHK(cudaMemcpy(host24[i], *state_ptr(i), g.bytes, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int ymref_step(int nsteps) {
+  if (!g.live) return YMKH_ESTATE;
+  for (int s = 0; s < nsteps; ++s) {
+    int rc = step_once();
+    if (rc) return rc;
+  }
+  RCHK(cudaDeviceSynchronize());
+  return 0;
+}
+
+// ymgpu2d/YM_Energy.cu:23-32 unchanged (device per-cell energy, host sum).
+int ymref_energy(double* out) {
+  if (!g.live) return YMKH_ESTATE;
+  *out = compute_ym_energy(g.f, g.flA, g.flB, g.ebuf, g.h_ebuf, g.nx, g.nz, bl2(), th2());
+  RLAUNCH("energy");
+  return 0;
+}
+
+// Device time of nsteps iterations, in milliseconds (CUDA events around the
+// loop on the legacy stream the reference uses).
+int ymref_time_steps(int nsteps, float* ms) {
+  if (!g.live) return YMKH_ESTATE;
+  cudaEvent_t a, b;
+  RCHK(cudaEventCreate(&a));
+  RCHK(cudaEventCreate(&b));
+  RCHK(cudaDeviceSynchronize());
+  RCHK(cudaEventRecord(a, 0));
+  for (int s = 0; s < nsteps; ++s) {
+    int rc = step_once();
+    if (rc) return rc;
+  }
+  RCHK(cudaEventRecord(b, 0));
+  RCHK(cudaEventSynchronize(b));
+  RCHK(cudaEventElapsedTime(ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return 0;
+}
+
+}  // extern "C"
