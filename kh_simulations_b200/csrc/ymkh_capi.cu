@@ -71,7 +71,9 @@ struct ymkh_ctx {
   double* epart = nullptr;   // energy partials
   double* edev = nullptr;    // [0] energy, [1..2] mode amplitudes
   double* mcol = nullptr;    // mode amplitude per-column buffer
-  int fct_tx = 64, fct_seg = 16;
+  int fct_tx = 64, fct_seg = 16, fct_grid = 296;  // FCT threads per beam, segment rows, persistent CTAs
+  int mx_seg = 16, mx_grid = 148;                   // Maxwell segment rows, persistent CTAs
+  int sms = 148;
   // CUDA graphs of `graph_steps` steps, one per starting buffer
   int graph_steps = 4;
   cudaGraphExec_t gexec[2]{nullptr, nullptr};
@@ -147,15 +149,32 @@ int setup_params(ymkh_ctx* c, const ymkh_params* p) {
   return 0;
 }
 
+// Segment length for persistent CTAs taking (strip, segment) items
+// round-robin: the smallest per-CTA item count whose last round is nearly
+// full, with segments of at least 16 rows.
+int pick_segment(int nz, int nstrips, int grid) {
+  int best_seg = nz, best_cost = 1 << 30;
+  for (int nseg = 1; nseg <= std::max(1, nz / 16); ++nseg) {
+    const int seg = (nz + nseg - 1) / nseg;
+    const int items = nstrips * ((nz + seg - 1) / seg);
+    const int rounds = (items + grid - 1) / grid;
+    // cost in rows per CTA, each item paying its 6-row start-up
+    const int cost = rounds * (seg + 6);
+    if (cost < best_cost) { best_cost = cost; best_seg = seg; }
+  }
+  return best_seg;
+}
+
 void choose_launch_shape(ymkh_ctx* c) {
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-  c->fct_tx = c->nx >= 64 ? 64 : 32;
-  const int strips = (c->nx + c->fct_tx - 1) / c->fct_tx;
-  const int target = 4 * sms;  // 2 CTAs per SM, two waves
-  int segs = std::max(1, (target + strips - 1) / strips);
-  int seg = (c->nz + segs - 1) / segs;
-  c->fct_seg = std::max(16, seg);
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
+  c->fct_tx = c->nx >= 128 ? 64 : 32;
+  const int fct_per_sm = std::max(1, fct_ctas_per_sm(c->fct_tx));
+  c->fct_grid = c->sms * fct_per_sm;
+  const int fstrips = (c->nx + (c->fct_tx - 4) - 1) / (c->fct_tx - 4);
+  c->fct_seg = pick_segment(c->nz, fstrips, c->fct_grid);
+  const int mx_per_sm = std::max(1, maxwell_ctas_per_sm());
+  c->mx_grid = c->sms * mx_per_sm;
+  c->mx_seg = pick_segment(c->nz, (c->nx + 127) / 128, c->mx_grid);
 }
 
 ArrayList list21(const State& s) {
@@ -185,9 +204,9 @@ int step_once(ymkh_ctx* c, cudaStream_t s) {
   const State& in = c->buf[c->cur];
   const State& out = c->buf[1 - c->cur];
   mark(c, ST_FCT, s);
-  CK(launch_fct(in, out, c->sp, c->fct_tx, c->fct_seg, s), "fct_fused_kernel");
+  CK(launch_fct(in, out, c->sp, c->fct_tx, c->fct_seg, c->fct_grid, s), "fct_fused_kernel");
   mark(c, ST_MAXWELL, s);
-  CK(launch_maxwell(out, in, out, c->sp, s), "maxwell_fused_kernel");
+  CK(launch_maxwell(out, in, out, c->sp, c->mx_seg, c->mx_grid, s), "maxwell_fused_kernel");
   mark(c, ST_POINTWISE, s);
   g_launches += 2;
   if (c->prm.xi_sponge > 0.0) { CK(launch_sponge_xicut(list12(out), c->sp, 0, s), "sponge"); g_launches++; }
@@ -279,8 +298,11 @@ int ymkh_create(const ymkh_grid* grid, const ymkh_params* params, ymkh_ctx** out
   c->nx = grid->nx; c->nz = grid->nz; c->N = (size_t)grid->nx * grid->nz;
   int rc = setup_params(c, params);
   if (rc) { free_bands(c); delete c; return rc; }
+  CK(prepare_fct(32), "FCT kernel attributes");
+  CK(prepare_fct(64), "FCT kernel attributes");
+  CK(prepare_fct(128), "FCT kernel attributes");
+  CK(prepare_maxwell(), "Maxwell kernel attributes");
   choose_launch_shape(c);
-  CK(prepare_fct(c->fct_tx), "FCT kernel attributes");
   CK(prepare_column(c->nz), "column kernel attributes");
   const int np = energy_nparts(c->N);
   if (cudaMalloc(&c->epart, (size_t)2 * np * sizeof(double)) != cudaSuccess ||
@@ -431,9 +453,9 @@ int ymkh_set_graph_steps(ymkh_ctx* c, int n) {
 int ymkh_set_fct_shape(ymkh_ctx* c, int tx, int seg) {
   if (!c || (tx != 32 && tx != 64 && tx != 128) || seg < 1) return set_err(YMKH_EINVAL, "bad FCT launch shape");
   drop_graphs(c);
-  CK(prepare_fct(tx), "FCT kernel attributes");
   c->fct_tx = tx;
   c->fct_seg = seg;
+  c->fct_grid = c->sms * std::max(1, fct_ctas_per_sm(tx));
   return 0;
 }
 

@@ -7,6 +7,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <algorithm>
 #include "../../include/ymkh.h"
 
 namespace ymkh {
@@ -107,10 +108,14 @@ struct InitArgs {
 
 // Launchers (one per kernel family).  prepare_* set function attributes
 // outside any stream capture.
-cudaError_t prepare_fct(int tx);
-cudaError_t launch_fct(const State& in, const State& out, const StepParams& p, int tx, int seg_len, cudaStream_t s);
+cudaError_t prepare_fct(int tb);
+int fct_ctas_per_sm(int tb);
+cudaError_t launch_fct(const State& in, const State& out, const StepParams& p, int tb, int seg_len, int grid_ctas,
+                       cudaStream_t s);
+cudaError_t prepare_maxwell();
+int maxwell_ctas_per_sm();
 cudaError_t launch_maxwell(const State& fluid_new, const State& fields_old, const State& out, const StepParams& p,
-                           cudaStream_t s);
+                           int seg_len, int grid_ctas, cudaStream_t s);
 cudaError_t launch_sponge_xicut(const ArrayList& a12, const StepParams& p, int cut, cudaStream_t s);
 cudaError_t prepare_column(int nz);
 cudaError_t launch_zmean(const ArrayList& a15, int nx, int nz, cudaStream_t s);

@@ -11,10 +11,13 @@
 // kernel_ym_precession, YM_Fluid.cu:32-108) are recomputed here from the
 // start-of-step state, which is what they are a function of.
 //
-// Layout: a CTA owns an x-strip [x0, x0+TX) and a z-segment [zs, ze) and
-// streams along z.  Threads [0,TX) handle beam A, [TX,2TX) beam B.  Row data
-// (12 fluid arrays plus the field rows the sources need) is staged into
-// shared memory with cp.async NST-1 rows ahead.  For each row the x-sweep
+// Layout: work items are (x-strip, z-segment) pairs, handed to persistent
+// CTAs round-robin.  A strip emits TB-4 columns [x0, x0+TB-4); thread t of a
+// beam owns x-sweep position x0-2+t, so every x-sweep phase is exactly one
+// position per thread.  Threads [0,TB) handle beam A, [TB,2TB) beam B; the
+// beams synchronise only through their own named barriers.  Row data (12
+// fluid arrays plus the field rows the sources need) is staged in shared
+// memory with cp.async NST-1 rows ahead.  For each row the x-sweep
 // (FCT_Sweeps.cu:88-162) runs across the strip in shared memory; its result
 // for the thread's own column feeds a register pipeline that performs the
 // z-sweep along the stream, emitting row r-3 once row r arrives (halo 3,
@@ -29,329 +32,336 @@ namespace ymkh {
 
 namespace {
 
-// Offsets (in units of W doubles) inside one stage buffer.
-constexpr int ST_FL = 0;     // fluid: (beam*6 + var)
-constexpr int ST_EX = 12;    // Ex1..3, row zr
-constexpr int ST_BY = 15;    // By1..3, row zr
-constexpr int ST_BYM = 18;   // By1..3, row zm
-constexpr int ST_EZ = 21;    // Ez1..3, row zr
-constexpr int ST_EZM = 24;   // Ez1..3, row zm
-constexpr int ST_AZ = 27;    // Az1..3, row zr
-constexpr int ST_AZM = 30;   // Az1..3, row zm
-constexpr int ST_NZP = 33;   // n (beam A, B), row zp (warm_T only)
-constexpr int ST_NZM = 35;   // n (beam A, B), row zm (warm_T only)
+// Offsets (in units of W doubles) inside one stage buffer; stage position
+// sp holds shear index x = x0 - 4 + sp.
+constexpr int ST_FL = 0;     // fluid: (beam*6 + var), sp in [1, TB+3)
+constexpr int ST_EX = 12;    // Ex1..3 row zr,         sp in [1, TB+2)
+constexpr int ST_BY = 15;    // By1..3 row zr,         sp in [1, TB+2)
+constexpr int ST_BYM = 18;   // By1..3 row zm,         sp in [1, TB+2)
+constexpr int ST_EZ = 21;    // Ez1..3 row zr,         sp in [4, TB)
+constexpr int ST_EZM = 24;   // Ez1..3 row zm
+constexpr int ST_AZ = 27;    // Az1..3 row zr
+constexpr int ST_AZM = 30;   // Az1..3 row zm
+constexpr int ST_NZP = 33;   // n (beam A, B) row zp (warm_T only)
+constexpr int ST_NZM = 35;   // n (beam A, B) row zm (warm_T only)
 constexpr int ST_SIZE = 37;
 
-// Work arrays (units of W): beam-shared node fields, then per beam.
-constexpr int WK_EXN = 0, WK_BYN = 3, WK_EZN = 6, WK_AZN = 9, WK_SHARED = 12;
-constexpr int WB_U = 0, WB_VZ = 1, WB_S = 2, WB_LOR = 3, WB_LNR = 9, WB_FLIM = 15, WB_SIZE = 21;
+// Per-beam work arrays (units of W), indexed by stage position.
+constexpr int WB_U = 0, WB_LOR = 1, WB_LNR = 7, WB_FLIM = 13, WB_SIZE = 19;
+
+__device__ __forceinline__ void beam_bar(int beam, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(beam + 1), "r"(nthreads) : "memory");
+}
 
 }  // namespace
 
-template <int TX>
+template <int TB>
 constexpr size_t fct_smem_bytes(int nst) {
-  return (size_t)(TX + 8) * sizeof(double) * (nst * ST_SIZE + WK_SHARED + 2 * WB_SIZE) +
-         (size_t)(TX + 8) * sizeof(int);
+  return (size_t)(TB + 4) * sizeof(double) * (nst * ST_SIZE + 2 * WB_SIZE) + (size_t)(TB + 4) * sizeof(int);
 }
 
-template <int TX, int NST>
-__global__ void __launch_bounds__(2 * TX)
+struct FctSched {
+  int nstrips;   // strips of TB-4 output columns
+  int seg_len;   // rows per z-segment
+  int nitems;    // nstrips * nsegments
+};
+
+template <int TB, int NST>
+__global__ void __launch_bounds__(2 * TB)
     fct_fused_kernel(const __grid_constant__ State st, const __grid_constant__ State out,
-                     const __grid_constant__ StepParams p, int seg_len) {
-  constexpr int W = TX + 8;
-  constexpr int NT = 2 * TX;
+                     const __grid_constant__ StepParams p, const FctSched sc) {
+  constexpr int W = TB + 4;
+  constexpr int NT = 2 * TB;
+  constexpr int TO = TB - 4;  // output columns per strip
   extern __shared__ __align__(16) double smem[];
-  double* stage = smem;
-  double* wk = smem + (size_t)NST * ST_SIZE * W;
-  int* xtab = reinterpret_cast<int*>(wk + (size_t)(WK_SHARED + 2 * WB_SIZE) * W);
+  double* const stage = smem;
+  double* const wk = smem + (size_t)NST * ST_SIZE * W;
+  int* const xtab = reinterpret_cast<int*>(wk + (size_t)2 * WB_SIZE * W);
 
   const int nx = p.nx, nz = p.nz;
   const int tid = threadIdx.x;
-  const int beam = tid / TX;
-  const int t = tid - beam * TX;
-  const int x0 = blockIdx.x * TX;
-  const int zs = blockIdx.y * seg_len;
-  const int ze = min(nz, zs + seg_len);
-  if (zs >= nz) return;
+  const int beam = tid / TB;
+  const int t = tid - beam * TB;
+  const int sp = t + 2;  // stage position of this thread's x-sweep position
   const bool warm = p.warm_T > 0.0;
+  const bool wall = !p.periodic_x;
   const double dt = p.dt;
   const double dtdx = p.dt / p.dx;
   const double dtdz = p.dt / p.dz;
+  double* const wb = wk + (size_t)beam * WB_SIZE * W;
 
-  // Mapped shear index of every stage position p <-> x = x0 - 4 + p.
-  for (int i = tid; i < W; i += NT) xtab[i] = xmap(x0 - 4 + i, nx, p.periodic_x);
-  __syncthreads();
+  for (int item = blockIdx.x; item < sc.nitems; item += gridDim.x) {
+    const int strip = item % sc.nstrips;
+    const int x0 = strip * TO;
+    const int zs = (item / sc.nstrips) * sc.seg_len;
+    const int ze = min(nz, zs + sc.seg_len);
 
-  auto issue_row = [&](int r, int s) {
-    double* sb = stage + (size_t)s * ST_SIZE * W;
-    const int zr = zclamp(r, nz);
-    const int zm = (zr == 0) ? nz - 1 : zr - 1;
-    const int zp = (zr == nz - 1) ? 0 : zr + 1;
-    const size_t ro = (size_t)zr * nx, rom = (size_t)zm * nx, rop = (size_t)zp * nx;
-    // 12 fluid rows, positions [1, TX+7)
-    for (int i = tid; i < 12 * (TX + 6); i += NT) {
-      const int a = i / (TX + 6), q = i - a * (TX + 6);
-      const double* src = (a < 6 ? st.a[a] : st.b[a - 6]) + ro + xtab[1 + q];
-      cp_async8(sb + (ST_FL + a) * W + 1 + q, src);
-    }
-    // Ex (zr), By (zr), By (zm), positions [1, TX+6)
-    for (int i = tid; i < 9 * (TX + 5); i += NT) {
-      const int a = i / (TX + 5), q = i - a * (TX + 5);
-      const int c = a % 3;
-      const double* base = (a < 3) ? st.f[EX1 + c] : st.f[BY1 + c];
-      const double* src = base + (a < 6 ? ro : rom) + xtab[1 + q];
-      cp_async8(sb + (ST_EX + a) * W + 1 + q, src);
-    }
-    // Ez (zr, zm), Az (zr, zm), positions [4, TX+4)
-    for (int i = tid; i < 12 * TX; i += NT) {
-      const int a = i / TX, q = i - a * TX;
-      const int c = a % 3, kind = a / 3;
-      const double* base = (kind < 2) ? st.f[EZ1 + c] : st.f[AZ1 + c];
-      const double* src = base + ((kind & 1) ? rom : ro) + xtab[4 + q];
-      cp_async8(sb + (ST_EZ + a) * W + 4 + q, src);
-    }
-    if (warm) {
-      for (int i = tid; i < 4 * TX; i += NT) {
-        const int a = i / TX, q = i - a * TX;
-        const double* base = (a & 1) ? st.b[FN] : st.a[FN];
-        const double* src = base + ((a >> 1) ? rom : rop) + xtab[4 + q];
-        cp_async8(sb + (ST_NZP + a) * W + 4 + q, src);
+    __syncthreads();  // previous item fully consumed
+    for (int i = tid; i < W; i += NT) xtab[i] = xmap(x0 - 4 + i, nx, p.periodic_x);
+    __syncthreads();
+
+    auto issue_row = [&](int r, int s) {
+      double* sb = stage + (size_t)s * ST_SIZE * W;
+      const int zr = zclamp(r, nz);
+      const int zm = (zr == 0) ? nz - 1 : zr - 1;
+      const int zp = (zr == nz - 1) ? 0 : zr + 1;
+      const size_t ro = (size_t)zr * nx, rom = (size_t)zm * nx, rop = (size_t)zp * nx;
+      for (int i = tid; i < 12 * (TB + 2); i += NT) {
+        const int a = i / (TB + 2), q = i - a * (TB + 2);
+        const double* src = (a < 6 ? st.a[a] : st.b[a - 6]) + ro + xtab[1 + q];
+        cp_async8(sb + (ST_FL + a) * W + 1 + q, src);
       }
-    }
-  };
+      for (int i = tid; i < 9 * (TB + 1); i += NT) {
+        const int a = i / (TB + 1), q = i - a * (TB + 1);
+        const int c = a % 3;
+        const double* base = (a < 3) ? st.f[EX1 + c] : st.f[BY1 + c];
+        cp_async8(sb + (ST_EX + a) * W + 1 + q, base + (a < 6 ? ro : rom) + xtab[1 + q]);
+      }
+      for (int i = tid; i < 12 * TO; i += NT) {
+        const int a = i / TO, q = i - a * TO;
+        const int c = a % 3, kind = a / 3;
+        const double* base = (kind < 2) ? st.f[EZ1 + c] : st.f[AZ1 + c];
+        cp_async8(sb + (ST_EZ + a) * W + 4 + q, base + ((kind & 1) ? rom : ro) + xtab[4 + q]);
+      }
+      if (warm) {
+        for (int i = tid; i < 4 * TO; i += NT) {
+          const int a = i / TO, q = i - a * TO;
+          const double* base = (a & 1) ? st.b[FN] : st.a[FN];
+          cp_async8(sb + (ST_NZP + a) * W + 4 + q, base + ((a >> 1) ? rom : rop) + xtab[4 + q]);
+        }
+      }
+    };
 
-  const int r_first = zs - 3, r_last = ze + 2;
-  // prologue: NST-1 rows in flight
+    const int r_first = zs - 3, r_last = ze + 2;
 #pragma unroll
-  for (int k = 0; k < NST - 1; ++k) {
-    if (r_first + k <= r_last) issue_row(r_first + k, k);
-    cp_async_commit();
-  }
-
-  // z-pipeline registers (see header comment); index k = swept variable.
-  double V1[6], f1[6], d1[6], L2[6], N4[6], N3[6], N2[6], A2[6], F3[6], S1[6];
-#pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    V1[k] = f1[k] = d1[k] = L2[k] = N4[k] = N3[k] = N2[k] = A2[k] = F3[k] = S1[k] = 0.0;
-  }
-  double U1 = 0.0, mu1 = 0.0;
-
-  double* const xn = wk;                                   // beam-shared node fields
-  double* const wb = wk + (size_t)(WK_SHARED + beam * WB_SIZE) * W;  // this beam
-  const int x_own = x0 + t;
-  const bool wall = !p.periodic_x;
-
-  for (int r = r_first, it = 0; r <= r_last; ++r, ++it) {
-    __syncthreads();  // every thread is done with the stage about to be refilled
-    {
-      const int rn = r + NST - 1;
-      if (rn <= r_last) issue_row(rn, (it + NST - 1) % NST);
+    for (int k = 0; k < NST - 1; ++k) {
+      if (r_first + k <= r_last) issue_row(r_first + k, k);
       cp_async_commit();
     }
-    cp_async_wait<NST - 1>();
-    __syncthreads();
-    const double* sb = stage + (size_t)(it % NST) * ST_SIZE * W;
-    const double* fl = sb + (size_t)(ST_FL + beam * 6) * W;
 
-    // ---- Phase A: velocities (YM_Fluid.cu:3-11) and node-centred fields.
-    for (int q = t; q < TX + 6; q += TX) {
-      const int pp = 1 + q;
-      const double ns = fmax(fl[FN * W + pp], 0.05);
-      wb[WB_U * W + pp] = fl[FPX * W + pp] / ns;
-      wb[WB_VZ * W + pp] = fl[FPZ * W + pp] / ns;
-    }
-    for (int i = tid; i < (TX + 4) + TX; i += NT) {
-      if (i < TX + 4) {
-        const int pp = 2 + i;
+    double V1[6], f1[6], d1[6], L2[6], N4[6], N3[6], N2[6], A2[6], F3[6], S1[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) V1[k] = f1[k] = d1[k] = L2[k] = N4[k] = N3[k] = N2[k] = A2[k] = F3[k] = S1[k] = 0.0;
+    double U1 = 0.0, mu1 = 0.0;
+    const int x_own = x0 - 2 + t;
+    const bool owner = (t >= 2) && (t < TB - 2) && (x_own < nx);
+
+    for (int r = r_first, it = 0; r <= r_last; ++r, ++it) {
+      cp_async_wait<NST - 2>();
+      __syncthreads();  // row r staged by every thread; row r-1's stage is free
+      {
+        const int rn = r + NST - 1;
+        if (rn <= r_last) issue_row(rn, (it + NST - 1) % NST);
+        cp_async_commit();
+      }
+      const double* sb = stage + (size_t)(it % NST) * ST_SIZE * W;
+      const double* fl = sb + (size_t)(ST_FL + beam * 6) * W;
+
+      // ---- A: velocities (YM_Fluid.cu:3-11) at sp (and the two edge
+      // positions), px source (YM_Fluid.cu:43-66, 71-80) at sp.
+      double vz_own;
+      {
+        const double ns = fmax(fl[FN * W + sp], 0.05);
+        wb[WB_U * W + sp] = fl[FPX * W + sp] / ns;
+        vz_own = fl[FPZ * W + sp] / ns;
+        if (t == 0 || t == TB - 1) {
+          const int e = (t == 0) ? 1 : TB + 2;
+          const double ne = fmax(fl[FN * W + e], 0.05);
+          wb[WB_U * W + e] = fl[FPX * W + e] / ne;
+        }
+      }
+      double sx;
+      {
+        int ps = sp;  // at a wall the clamped ghost cells carry the edge cell's source
+        if (wall) {
+          const int xg = x0 - 4 + sp;
+          ps = (xg < 0 ? 0 : (xg >= nx ? nx - 1 : xg)) - (x0 - 4);
+        }
+        const double vz = (ps == sp) ? vz_own : fl[FPZ * W + ps] / fmax(fl[FN * W + ps], 0.05);
+        double acc;
+        {
+          const double ex = 0.5 * (sb[(ST_EX + 0) * W + ps] + sb[(ST_EX + 0) * W + ps - 1]);
+          const double by = 0.25 * (sb[(ST_BY + 0) * W + ps] + sb[(ST_BY + 0) * W + ps - 1] +
+                                    sb[(ST_BYM + 0) * W + ps] + sb[(ST_BYM + 0) * W + ps - 1]);
+          acc = fl[FQ1 * W + ps] * (ex + vz * by);
+        }
+#pragma unroll
+        for (int c = 1; c < 3; ++c) {
+          const double ex = 0.5 * (sb[(ST_EX + c) * W + ps] + sb[(ST_EX + c) * W + ps - 1]);
+          const double by = 0.25 * (sb[(ST_BY + c) * W + ps] + sb[(ST_BY + c) * W + ps - 1] +
+                                    sb[(ST_BYM + c) * W + ps] + sb[(ST_BYM + c) * W + ps - 1]);
+          acc = acc + fl[(FQ1 + c) * W + ps] * (ex + vz * by);
+        }
+        sx = -acc;
+        if (warm) {
+          const double dndx = (fl[FN * W + ps + 1] - fl[FN * W + ps - 1]) / (2.0 * p.dx);
+          sx -= p.warm_T * dndx;
+        }
+      }
+      beam_bar(beam, TB);
+
+      // ---- B: x-sweep low-order solution at sp (FCT_Sweeps.cu:88-133).
+      {
+        const double um = wb[WB_U * W + sp - 1], u0 = wb[WB_U * W + sp], up = wb[WB_U * W + sp + 1];
+        const double eL = fct_eps(um, u0, dtdx), eR = fct_eps(u0, up, dtdx);
+        double nuL, muL, nuR, muR;
+        fct_nu_mu(eL, nuL, muL);
+        fct_nu_mu(eR, nuR, muR);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          const double vm = fl[k * W + sp - 1], v0 = fl[k * W + sp], vp = fl[k * W + sp + 1];
+          const double fL = 0.5 * eL * (vm + v0);
+          const double fR = 0.5 * eR * (v0 + vp);
+          const double dL = nuL * (v0 - vm);
+          const double dR = nuR * (vp - v0);
+          const double lo = (k == FPX) ? v0 + dt * sx - (fR - fL) : v0 - (fR - fL);
+          wb[(WB_LOR + k) * W + sp] = lo;
+          wb[(WB_LNR + k) * W + sp] = lo + (dR - dL);
+        }
+      }
+      beam_bar(beam, TB);
+
+      // ---- C: antidiffusive flux and limiter at interface sp+1/2
+      // (FCT_Sweeps.cu:139-160), t in [1, TB-2).
+      if (t >= 1 && t < TB - 2) {
+        const double e = fct_eps(wb[WB_U * W + sp], wb[WB_U * W + sp + 1], dtdx);
+        double nu, mu;
+        fct_nu_mu(e, nu, mu);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          const double* lor = wb + (WB_LOR + k) * W;
+          const double* lnr = wb + (WB_LNR + k) * W;
+          const double fad = mu * (lor[sp + 1] - lor[sp]);
+          wb[(WB_FLIM + k) * W + sp] =
+              fct_limit(fad, lnr[sp] - lnr[sp - 1], lnr[sp + 1] - lnr[sp], lnr[sp + 2] - lnr[sp + 1]);
+        }
+      }
+      beam_bar(beam, TB);
+
+      // ---- D: x-swept value of the own column, z-sources, z-pipeline.
+      if (t >= 2 && t < TB - 2) {
+        double Vx[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+          Vx[k] = wb[(WB_LNR + k) * W + sp] - (wb[(WB_FLIM + k) * W + sp] - wb[(WB_FLIM + k) * W + sp - 1]);
+        const double vx = wb[WB_U * W + sp];
+        const double vz = vz_own;
+        const double q1 = fl[FQ1 * W + sp], q2 = fl[FQ2 * W + sp], q3 = fl[FQ3 * W + sp];
+        double by[3], ezn[3], azn[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          const double* ex = sb + (ST_EX + c) * W;
-          const double* by = sb + (ST_BY + c) * W;
-          const double* bym = sb + (ST_BYM + c) * W;
-          // YM_Fluid.cu:48-62
-          xn[(WK_EXN + c) * W + pp] = 0.5 * (ex[pp] + ex[pp - 1]);
-          xn[(WK_BYN + c) * W + pp] = 0.25 * (by[pp] + by[pp - 1] + bym[pp] + bym[pp - 1]);
+          by[c] = 0.25 * (sb[(ST_BY + c) * W + sp] + sb[(ST_BY + c) * W + sp - 1] + sb[(ST_BYM + c) * W + sp] +
+                          sb[(ST_BYM + c) * W + sp - 1]);
+          ezn[c] = 0.5 * (sb[(ST_EZ + c) * W + sp] + sb[(ST_EZM + c) * W + sp]);
+          azn[c] = 0.5 * (sb[(ST_AZ + c) * W + sp] + sb[(ST_AZM + c) * W + sp]);
         }
-      } else {
-        const int pp = 4 + (i - (TX + 4));
+        // YM_Fluid.cu:67 (src.pz) and :76-79 (warm closure)
+        double sz = -(q1 * (ezn[0] - vx * by[0]) + q2 * (ezn[1] - vx * by[1]) + q3 * (ezn[2] - vx * by[2]));
+        if (warm) {
+          const double dndz = (sb[(ST_NZP + beam) * W + sp] - sb[(ST_NZM + beam) * W + sp]) / (2.0 * p.dz);
+          sz -= p.warm_T * dndz;
+        }
+        // YM_Fluid.cu:99-107 (colour precession)
+        double S[6];
+        S[FN] = 0.0;
+        S[FPX] = 0.0;
+        S[FPZ] = sz;
+        S[FQ1] = p.alpha * vz * (q2 * azn[2] - q3 * azn[1]);
+        S[FQ2] = p.alpha * vz * (q3 * azn[0] - q1 * azn[2]);
+        S[FQ3] = p.alpha * vz * (q1 * azn[1] - q2 * azn[0]);
+
+        const double e = fct_eps(U1, vz, dtdz);
+        double nu, mu;
+        fct_nu_mu(e, nu, mu);
+        double outv[6];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          xn[(WK_EZN + c) * W + pp] = 0.5 * (sb[(ST_EZ + c) * W + pp] + sb[(ST_EZM + c) * W + pp]);
-          xn[(WK_AZN + c) * W + pp] = 0.5 * (sb[(ST_AZ + c) * W + pp] + sb[(ST_AZM + c) * W + pp]);
+        for (int k = 0; k < 6; ++k) {
+          const double fR = 0.5 * e * (V1[k] + Vx[k]);
+          const double dR = nu * (Vx[k] - V1[k]);
+          const double lo = (k >= FPZ) ? V1[k] + dt * S1[k] - (fR - f1[k]) : V1[k] - (fR - f1[k]);
+          const double ln = lo + (dR - d1[k]);
+          const double fad = mu1 * (lo - L2[k]);
+          const double flim = fct_limit(A2[k], N3[k] - N4[k], N2[k] - N3[k], ln - N2[k]);
+          outv[k] = N3[k] - (flim - F3[k]);
+          V1[k] = Vx[k];
+          S1[k] = S[k];
+          f1[k] = fR;
+          d1[k] = dR;
+          L2[k] = lo;
+          N4[k] = N3[k];
+          N3[k] = N2[k];
+          N2[k] = ln;
+          A2[k] = fad;
+          F3[k] = flim;
+        }
+        U1 = vz;
+        mu1 = mu;
+        const int o = r - 3;
+        if (owner && o >= zs && o < ze) {
+          // YM_Fluid.cu:20-29 (density floor, wall momentum)
+          if (outv[FN] < 0.05) outv[FN] = 0.05;
+          if (wall && (x_own == 0 || x_own == nx - 1)) outv[FPX] = 0.0;
+          double* const* dst = beam ? out.b : out.a;
+          const size_t gi = idx2(x_own, o, nx);
+#pragma unroll
+          for (int k = 0; k < 6; ++k) dst[k][gi] = outv[k];
         }
       }
     }
-    __syncthreads();
-
-    // ---- Phase B: x-sweep low-order solution (FCT_Sweeps.cu:88-133) at
-    // positions [2, TX+6); the px source is kernel_ym_lorentz's src.px.
-    for (int q = t; q < TX + 4; q += TX) {
-      const int pp = 2 + q;
-      int ps = pp;  // source cell: clamped ends evaluate the edge cell's source
-      if (wall) {
-        const int xg = x0 - 4 + pp;
-        const int xc = xg < 0 ? 0 : (xg >= nx ? nx - 1 : xg);
-        ps = xc - (x0 - 4);
-      }
-      const double vz = wb[WB_VZ * W + ps];
-      double sx = -(fl[FQ1 * W + ps] * (xn[(WK_EXN + 0) * W + ps] + vz * xn[(WK_BYN + 0) * W + ps]) +
-                    fl[FQ2 * W + ps] * (xn[(WK_EXN + 1) * W + ps] + vz * xn[(WK_BYN + 1) * W + ps]) +
-                    fl[FQ3 * W + ps] * (xn[(WK_EXN + 2) * W + ps] + vz * xn[(WK_BYN + 2) * W + ps]));
-      if (warm) {
-        const double dndx = (fl[FN * W + ps + 1] - fl[FN * W + ps - 1]) / (2.0 * p.dx);
-        sx -= p.warm_T * dndx;
-      }
-      wb[WB_S * W + pp] = sx;
-      const double um = wb[WB_U * W + pp - 1], u0 = wb[WB_U * W + pp], up = wb[WB_U * W + pp + 1];
-      const double eL = fct_eps(um, u0, dtdx), eR = fct_eps(u0, up, dtdx);
-      double nuL, muL, nuR, muR;
-      fct_nu_mu(eL, nuL, muL);
-      fct_nu_mu(eR, nuR, muR);
-#pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        const double vm = fl[k * W + pp - 1], v0 = fl[k * W + pp], vp = fl[k * W + pp + 1];
-        const double fL = 0.5 * eL * (vm + v0);
-        const double fR = 0.5 * eR * (v0 + vp);
-        const double dL = nuL * (v0 - vm);
-        const double dR = nuR * (vp - v0);
-        double lo;
-        if (k == FPX)
-          lo = v0 + dt * sx - (fR - fL);
-        else
-          lo = v0 - (fR - fL);
-        wb[(WB_LOR + k) * W + pp] = lo;
-        wb[(WB_LNR + k) * W + pp] = lo + (dR - dL);
-      }
-    }
-    __syncthreads();
-
-    // ---- Phase C: antidiffusive fluxes and limiter at interfaces p+1/2,
-    // p in [3, TX+4) (FCT_Sweeps.cu:139-160).
-    for (int q = t; q < TX + 1; q += TX) {
-      const int pp = 3 + q;
-      const double e = fct_eps(wb[WB_U * W + pp], wb[WB_U * W + pp + 1], dtdx);
-      double nu, mu;
-      fct_nu_mu(e, nu, mu);
-#pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        const double* lor = wb + (WB_LOR + k) * W;
-        const double* lnr = wb + (WB_LNR + k) * W;
-        const double fad = mu * (lor[pp + 1] - lor[pp]);
-        wb[(WB_FLIM + k) * W + pp] =
-            fct_limit(fad, lnr[pp] - lnr[pp - 1], lnr[pp + 1] - lnr[pp], lnr[pp + 2] - lnr[pp + 1]);
-      }
-    }
-    __syncthreads();
-
-    // ---- Phase D: x-swept value of the own column, z-sources, z-pipeline.
-    {
-      const int pp = 4 + t;
-      double Vx[6];
-#pragma unroll
-      for (int k = 0; k < 6; ++k)
-        Vx[k] = wb[(WB_LNR + k) * W + pp] - (wb[(WB_FLIM + k) * W + pp] - wb[(WB_FLIM + k) * W + pp - 1]);
-      const double vx = wb[WB_U * W + pp];
-      const double vz = wb[WB_VZ * W + pp];
-      const double q1 = fl[FQ1 * W + pp], q2 = fl[FQ2 * W + pp], q3 = fl[FQ3 * W + pp];
-      const double by1 = xn[(WK_BYN + 0) * W + pp], by2 = xn[(WK_BYN + 1) * W + pp],
-                   by3 = xn[(WK_BYN + 2) * W + pp];
-      // YM_Fluid.cu:67 (src.pz) and :76-79 (warm closure)
-      double sz = -(q1 * (xn[(WK_EZN + 0) * W + pp] - vx * by1) + q2 * (xn[(WK_EZN + 1) * W + pp] - vx * by2) +
-                    q3 * (xn[(WK_EZN + 2) * W + pp] - vx * by3));
-      if (warm) {
-        const double dndz = (sb[(ST_NZP + beam) * W + pp] - sb[(ST_NZM + beam) * W + pp]) / (2.0 * p.dz);
-        sz -= p.warm_T * dndz;
-      }
-      // YM_Fluid.cu:99-107 (colour precession)
-      const double a1 = xn[(WK_AZN + 0) * W + pp], a2 = xn[(WK_AZN + 1) * W + pp], a3 = xn[(WK_AZN + 2) * W + pp];
-      double S[6];
-      S[FN] = 0.0;
-      S[FPX] = 0.0;
-      S[FPZ] = sz;
-      S[FQ1] = p.alpha * vz * (q2 * a3 - q3 * a2);
-      S[FQ2] = p.alpha * vz * (q3 * a1 - q1 * a3);
-      S[FQ3] = p.alpha * vz * (q1 * a2 - q2 * a1);
-
-      // z-sweep pipeline: interface r-1/2 now known.
-      const double e = fct_eps(U1, vz, dtdz);
-      double nu, mu;
-      fct_nu_mu(e, nu, mu);
-      const int o = r - 3;
-      const bool emit = (o >= zs) && (o < ze) && (x_own < nx);
-      double outv[6];
-#pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        const double fR = 0.5 * e * (V1[k] + Vx[k]);
-        const double dR = nu * (Vx[k] - V1[k]);
-        double lo;
-        if (k >= FPZ)
-          lo = V1[k] + dt * S1[k] - (fR - f1[k]);
-        else
-          lo = V1[k] - (fR - f1[k]);
-        const double ln = lo + (dR - d1[k]);
-        const double fad = mu1 * (lo - L2[k]);
-        const double flim = fct_limit(A2[k], N3[k] - N4[k], N2[k] - N3[k], ln - N2[k]);
-        outv[k] = N3[k] - (flim - F3[k]);
-        V1[k] = Vx[k];
-        S1[k] = S[k];
-        f1[k] = fR;
-        d1[k] = dR;
-        L2[k] = lo;
-        N4[k] = N3[k];
-        N3[k] = N2[k];
-        N2[k] = ln;
-        A2[k] = fad;
-        F3[k] = flim;
-      }
-      U1 = vz;
-      mu1 = mu;
-      if (emit) {
-        // YM_Fluid.cu:20-29 (density floor, wall momentum)
-        if (outv[FN] < 0.05) outv[FN] = 0.05;
-        if (wall && (x_own == 0 || x_own == nx - 1)) outv[FPX] = 0.0;
-        double* const* dst = beam ? out.b : out.a;
-        const size_t gi = idx2(x_own, o, nx);
-#pragma unroll
-        for (int k = 0; k < 6; ++k) dst[k][gi] = outv[k];
-      }
-    }
+    cp_async_wait<0>();
   }
-  cp_async_wait<0>();
+}
+
+template <int TB, int NST>
+static cudaError_t prepare_fct_t() {
+  return cudaFuncSetAttribute(fct_fused_kernel<TB, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)fct_smem_bytes<TB>(NST));
 }
 
 // The kernel reads start-of-step values across strip and segment halos while
 // other CTAs write theirs, so the fluid it writes goes to a second state
-// buffer (`out`); fields are only read.
-template <int TX, int NST>
-static cudaError_t prepare_fct_t() {
-  return cudaFuncSetAttribute(fct_fused_kernel<TX, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)fct_smem_bytes<TX>(NST));
-}
-
-template <int TX, int NST>
-static cudaError_t launch_fct_t(const State& in, const State& out, const StepParams& p, int seg_len,
+// buffer (`out`); fields are only read.  grid_ctas persistent CTAs take the
+// (strip, segment) items round-robin.
+template <int TB, int NST>
+static cudaError_t launch_fct_t(const State& in, const State& out, const StepParams& p, int seg_len, int grid_ctas,
                                 cudaStream_t s) {
-  const size_t smem = fct_smem_bytes<TX>(NST);
-  dim3 grid((p.nx + TX - 1) / TX, (p.nz + seg_len - 1) / seg_len);
-  fct_fused_kernel<TX, NST><<<grid, 2 * TX, smem, s>>>(in, out, p, seg_len);
+  FctSched sc;
+  sc.nstrips = (p.nx + (TB - 4) - 1) / (TB - 4);
+  sc.seg_len = seg_len;
+  sc.nitems = sc.nstrips * ((p.nz + seg_len - 1) / seg_len);
+  const int grid = std::min(sc.nitems, grid_ctas);
+  fct_fused_kernel<TB, NST><<<grid, 2 * TB, fct_smem_bytes<TB>(NST), s>>>(in, out, p, sc);
   return cudaGetLastError();
 }
 
-cudaError_t prepare_fct(int tx) {
-  switch (tx) {
-    case 32: return prepare_fct_t<32, 3>();
-    case 64: return prepare_fct_t<64, 3>();
-    case 128: return prepare_fct_t<128, 3>();
+constexpr int FCT_NST = 4;
+
+cudaError_t prepare_fct(int tb) {
+  switch (tb) {
+    case 32: return prepare_fct_t<32, FCT_NST>();
+    case 64: return prepare_fct_t<64, FCT_NST>();
+    case 128: return prepare_fct_t<128, FCT_NST>();
     default: return cudaErrorInvalidValue;
   }
 }
 
-cudaError_t launch_fct(const State& in, const State& out, const StepParams& p, int tx, int seg_len,
+int fct_ctas_per_sm(int tb) {
+  int n = 0;
+  switch (tb) {
+    case 32: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fct_fused_kernel<32, FCT_NST>, 64, fct_smem_bytes<32>(FCT_NST)); break;
+    case 64: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fct_fused_kernel<64, FCT_NST>, 128, fct_smem_bytes<64>(FCT_NST)); break;
+    case 128: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fct_fused_kernel<128, FCT_NST>, 256, fct_smem_bytes<128>(FCT_NST)); break;
+    default: break;
+  }
+  return n;
+}
+
+cudaError_t launch_fct(const State& in, const State& out, const StepParams& p, int tb, int seg_len, int grid_ctas,
                        cudaStream_t s) {
-  switch (tx) {
-    case 32: return launch_fct_t<32, 3>(in, out, p, seg_len, s);
-    case 64: return launch_fct_t<64, 3>(in, out, p, seg_len, s);
-    case 128: return launch_fct_t<128, 3>(in, out, p, seg_len, s);
+  switch (tb) {
+    case 32: return launch_fct_t<32, FCT_NST>(in, out, p, seg_len, grid_ctas, s);
+    case 64: return launch_fct_t<64, FCT_NST>(in, out, p, seg_len, grid_ctas, s);
+    case 128: return launch_fct_t<128, FCT_NST>(in, out, p, seg_len, grid_ctas, s);
     default: return cudaErrorInvalidValue;
   }
 }

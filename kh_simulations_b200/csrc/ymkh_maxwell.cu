@@ -3,187 +3,244 @@
 // One launch replaces stages 5-6 of the reference step
 // (ymgpu2d/main_ym.cu:357-363): colour currents (YM_Physics.cu:9-60),
 // Ampère (YM_Physics.cu:70-113), potential (YM_Physics.cu:589-599) and
-// Faraday (YM_Physics.cu:120-151).  The currents are never stored: each CTA
-// forms them from the new fluid for its tile plus a one-cell halo, updates E
-// on the tile plus the halo Faraday needs, then Az and By on the tile.
+// Faraday (YM_Physics.cu:120-151).  The currents are never stored.
 //
-// Reads the new fluid and the start-of-step fields from `in_*`, writes the
-// new E, By, Az to `out` (a different buffer: neighbouring tiles still read
-// the old values).  HBM per cell: 12 fluid + 12 field arrays read, 12 written.
+// Layout: work items are (x-strip of TX columns, z-segment) pairs handed to
+// persistent CTAs round-robin; a CTA streams along z with the rows it needs
+// staged in shared memory by cp.async NST-1 rows ahead.  When row q arrives
+// it forms, for every column, the per-cell velocities px/n and pz/n of both
+// beams (each division done once), then Ex(q) (Jx needs row q only) and
+// Ez(q-1) (Jz needs rows q-1, q), and finally the potential and Faraday on
+// row q-1, which need Ex at rows q-1, q and Ez at columns x, x+1.
+//
+// Reads the new fluid and the start-of-step fields from `in_*` and writes
+// E, By, Az to `out`, a different buffer (neighbouring CTAs still read the
+// old values).  HBM per cell: 24 arrays read, 12 written.
 
 #include "ymkh_common.cuh"
 
 namespace ymkh {
 
 namespace {
-constexpr int MX_TX = 32;
-constexpr int MX_TZ = 6;  // keeps the static shared tiles under 48 KB
+
+constexpr int MX_TX = 128;  // output columns per strip
+constexpr int MX_NT = 256;  // threads per CTA
+constexpr int MX_NST = 4;   // stage ring depth
+constexpr int MX_W = MX_TX + 2;  // stage row: position s <-> x = x0 - 1 + s
+
+// stage offsets in rows of MX_W doubles
+constexpr int MS_FL = 0;    // 12 fluid arrays, s in [1, TX+2)
+constexpr int MS_BY = 12;   // By1..3,          s in [0, TX+2)
+constexpr int MS_AZ = 15;   // Az1..3,          s in [1, TX+1)
+constexpr int MS_EX = 18;   // Ex1..3,          s in [1, TX+1)
+constexpr int MS_EZ = 21;   // Ez1..3,          s in [1, TX+2)
+constexpr int MS_SIZE = 24;
+
+// work rows: per-cell velocities [2 rows][beam][vx, vz], new Ex [2 rows][3], new Ez [3]
+constexpr int MW_V = 0;     // index (row&1)*4 + beam*2 + {0: px/n, 1: pz/n}
+constexpr int MW_EX = 8;    // (row&1)*3 + c
+constexpr int MW_EZ = 14;   // c
+constexpr int MW_SIZE = 17;
+
 }  // namespace
 
-__global__ void __launch_bounds__(MX_TX* MX_TZ)
+constexpr size_t maxwell_smem_bytes() {
+  return (size_t)MX_W * sizeof(double) * (MX_NST * MS_SIZE + MW_SIZE) + (size_t)MX_W * sizeof(int);
+}
+
+struct MxSched {
+  int nstrips, seg_len, nitems;
+};
+
+__global__ void __launch_bounds__(MX_NT)
     maxwell_fused_kernel(const __grid_constant__ State fluid_new, const __grid_constant__ State fields_old,
-                         const __grid_constant__ State out, const __grid_constant__ StepParams p) {
-  constexpr int TX = MX_TX, TZ = MX_TZ;
-  constexpr int FW = TX + 1, FH = TZ + 1;  // fluid tile   x in [x0, x0+TX], z in [z0, z0+TZ]
-  constexpr int BW = TX + 2, BH = TZ + 2;  // By tile      x in [x0-1, x0+TX], z in [z0-1, z0+TZ]
-  constexpr int AW = TX, AH = TZ + 1;      // Az, Ex tile  x in [x0, x0+TX), z in [z0, z0+TZ]
-  constexpr int EW = TX + 1, EH = TZ;      // Ez tile      x in [x0, x0+TX], z in [z0, z0+TZ)
-  __shared__ double s_fl[12][FH][FW];
-  __shared__ double s_by[3][BH][BW];
-  __shared__ double s_az[3][AH][AW];
-  __shared__ double s_ex[3][AH][AW];  // old, then new Ex
-  __shared__ double s_ez[3][EH][EW];  // old, then new Ez
+                         const __grid_constant__ State out, const __grid_constant__ StepParams p, const MxSched sc) {
+  constexpr int TX = MX_TX, W = MX_W, NST = MX_NST, NT = MX_NT;
+  extern __shared__ __align__(16) double smem[];
+  double* const stage = smem;
+  double* const wk = smem + (size_t)NST * MS_SIZE * W;
+  int* const xtab = reinterpret_cast<int*>(wk + (size_t)MW_SIZE * W);
 
   const int nx = p.nx, nz = p.nz;
-  const int x0 = blockIdx.x * TX, z0 = blockIdx.y * TZ;
   const int tid = threadIdx.x;
-  constexpr int NT = TX * TZ;
   const bool wall = !p.periodic_x;
-
-  for (int i = tid; i < 12 * FH * FW; i += NT) {
-    const int a = i / (FH * FW), r = i - a * FH * FW, zz = r / FW, xx = r - zz * FW;
-    const int gx = xmap(x0 + xx, nx, p.periodic_x), gz = zwrap(z0 + zz, nz);
-    const double* src = (a < 6) ? fluid_new.a[a] : fluid_new.b[a - 6];
-    s_fl[a][zz][xx] = src[idx2(gx, gz, nx)];
-  }
-  for (int i = tid; i < 3 * BH * BW; i += NT) {
-    const int c = i / (BH * BW), r = i - c * BH * BW, zz = r / BW, xx = r - zz * BW;
-    const int gx = xmap(x0 - 1 + xx, nx, p.periodic_x), gz = zwrap(z0 - 1 + zz, nz);
-    s_by[c][zz][xx] = fields_old.f[BY1 + c][idx2(gx, gz, nx)];
-  }
-  for (int i = tid; i < 3 * AH * AW; i += NT) {
-    const int c = i / (AH * AW), r = i - c * AH * AW, zz = r / AW, xx = r - zz * AW;
-    const int gx = xmap(x0 + xx, nx, p.periodic_x), gz = zwrap(z0 + zz, nz);
-    s_az[c][zz][xx] = fields_old.f[AZ1 + c][idx2(gx, gz, nx)];
-    s_ex[c][zz][xx] = fields_old.f[EX1 + c][idx2(gx, gz, nx)];
-  }
-  for (int i = tid; i < 3 * EH * EW; i += NT) {
-    const int c = i / (EH * EW), r = i - c * EH * EW, zz = r / EW, xx = r - zz * EW;
-    const int gx = xmap(x0 + xx, nx, p.periodic_x), gz = zwrap(z0 + zz, nz);
-    // YM_Fluid.cu:25-29: the wall boundary zeroes Ez before Ampère
-    const bool wz = wall && (gx == 0 || gx == nx - 1);
-    s_ez[c][zz][xx] = wz ? 0.0 : fields_old.f[EZ1 + c][idx2(gx, gz, nx)];
-  }
-  __syncthreads();
-
   const double dt = p.dt, c2 = p.c2, al = p.alpha, e0 = p.eps0;
-  // ---- Ampère for Ex on x in [x0, x0+TX), z in [z0, z0+TZ] (needs Jx).
-  double exn[3][2];
-#pragma unroll
-  for (int nex = 0; nex < 2; ++nex) {
-    const int i = tid + nex * NT;
-    if (i >= AW * AH) break;
-    const int zz = i / AW, xx = i - zz * AW;  // fluid (xx, zz) and (xx+1, zz)
-    double jx[3];
-    double nq[2][3], vxr[2];
-#pragma unroll
-    for (int b = 0; b < 2; ++b) {
-      const double n0 = s_fl[b * 6 + FN][zz][xx], np = s_fl[b * 6 + FN][zz][xx + 1];
-      vxr[b] = 0.5 * (s_fl[b * 6 + FPX][zz][xx] / fmax(n0, 1e-10) + s_fl[b * 6 + FPX][zz][xx + 1] / fmax(np, 1e-10));
-#pragma unroll
-      for (int a = 0; a < 3; ++a)
-        nq[b][a] = 0.5 * (n0 * s_fl[b * 6 + FQ1 + a][zz][xx] + np * s_fl[b * 6 + FQ1 + a][zz][xx + 1]);
-    }
-#pragma unroll
-    for (int a = 0; a < 3; ++a) jx[a] = -(nq[0][a] * vxr[0] + nq[1][a] * vxr[1]);
-    // By at (x, z) is s_by[zz+1][xx+1]; (x, zm) is s_by[zz][xx+1]
-    const double by1 = s_by[0][zz + 1][xx + 1], by2 = s_by[1][zz + 1][xx + 1], by3 = s_by[2][zz + 1][xx + 1];
-    const double d1 = (by1 - s_by[0][zz][xx + 1]) / p.dz;
-    const double d2 = (by2 - s_by[1][zz][xx + 1]) / p.dz;
-    const double d3 = (by3 - s_by[2][zz][xx + 1]) / p.dz;
-    const double a1 = s_az[0][zz][xx], a2 = s_az[1][zz][xx], a3 = s_az[2][zz][xx];
-    const double k1 = a2 * by3 - a3 * by2;
-    const double k2 = a3 * by1 - a1 * by3;
-    const double k3 = a1 * by2 - a2 * by1;
-    exn[0][nex] = s_ex[0][zz][xx] + dt * (c2 * (-d1 - al * k1) - jx[0] / e0);
-    exn[1][nex] = s_ex[1][zz][xx] + dt * (c2 * (-d2 - al * k2) - jx[1] / e0);
-    exn[2][nex] = s_ex[2][zz][xx] + dt * (c2 * (-d3 - al * k3) - jx[2] / e0);
-  }
-  // ---- Ampère for Ez on x in [x0, x0+TX], z in [z0, z0+TZ) (needs Jz).
-  double ezn[3][2];
-#pragma unroll
-  for (int nez = 0; nez < 2; ++nez) {
-    const int i = tid + nez * NT;
-    if (i >= EW * EH) break;
-    const int zz = i / EW, xx = i - zz * EW;  // fluid (xx, zz) and (xx, zz+1)
-    double nqz[2][3], vzt[2];
-#pragma unroll
-    for (int b = 0; b < 2; ++b) {
-      const double n0 = s_fl[b * 6 + FN][zz][xx], nzp = s_fl[b * 6 + FN][zz + 1][xx];
-      vzt[b] = 0.5 * (s_fl[b * 6 + FPZ][zz][xx] / fmax(n0, 1e-10) + s_fl[b * 6 + FPZ][zz + 1][xx] / fmax(nzp, 1e-10));
-#pragma unroll
-      for (int a = 0; a < 3; ++a)
-        nqz[b][a] = 0.5 * (n0 * s_fl[b * 6 + FQ1 + a][zz][xx] + nzp * s_fl[b * 6 + FQ1 + a][zz + 1][xx]);
-    }
-    const double by[3] = {s_by[0][zz + 1][xx + 1], s_by[1][zz + 1][xx + 1], s_by[2][zz + 1][xx + 1]};
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const double jz = -(nqz[0][a] * vzt[0] + nqz[1][a] * vzt[1]);
-      const double dbx = (by[a] - s_by[a][zz + 1][xx]) / p.dx;
-      ezn[a][nez] = s_ez[a][zz][xx] + dt * (c2 * dbx - jz / e0);
-    }
-  }
-  __syncthreads();  // all old Ex/Ez reads done
-#pragma unroll
-  for (int nex = 0; nex < 2; ++nex) {
-    const int i = tid + nex * NT;
-    if (i >= AW * AH) break;
-    const int zz = i / AW, xx = i - zz * AW;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) s_ex[a][zz][xx] = exn[a][nex];
-  }
-#pragma unroll
-  for (int nez = 0; nez < 2; ++nez) {
-    const int i = tid + nez * NT;
-    if (i >= EW * EH) break;
-    const int zz = i / EW, xx = i - zz * EW;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) s_ez[a][zz][xx] = ezn[a][nez];
-  }
-  __syncthreads();
-  // At a wall the right neighbour of the last column is the column itself
-  // (YM_Physics.cu:127), so the halo Ez is that column's new Ez.
-  if (wall && x0 + TX >= nx) {
-    for (int i = tid; i < 3 * EH; i += NT) {
-      const int a = i / EH, zz = i - a * EH;
-      const int xl = nx - 1 - x0;  // local index of the last real column
-      s_ez[a][zz][xl + 1] = s_ez[a][zz][xl];
-    }
-    __syncthreads();
-  }
 
-  // ---- Potential and Faraday on the tile.
-  {
-    const int zz = tid / TX, xx = tid - zz * TX;
-    const int gx = x0 + xx, gz = z0 + zz;
-    if (gx < nx && gz < nz) {
-      const size_t gi = idx2(gx, gz, nx);
-      double az[3];
+  for (int item = blockIdx.x; item < sc.nitems; item += gridDim.x) {
+    const int x0 = (item % sc.nstrips) * TX;
+    const int zs = (item / sc.nstrips) * sc.seg_len;
+    const int ze = min(nz, zs + sc.seg_len);
+
+    __syncthreads();
+    for (int i = tid; i < W; i += NT) xtab[i] = xmap(x0 - 1 + i, nx, p.periodic_x);
+    __syncthreads();
+
+    auto issue_row = [&](int q, int s) {
+      double* sb = stage + (size_t)s * MS_SIZE * W;
+      const size_t ro = (size_t)zwrap(q, nz) * nx;
+      for (int i = tid; i < 12 * (TX + 1); i += NT) {
+        const int a = i / (TX + 1), k = i - a * (TX + 1);
+        const double* src = (a < 6 ? fluid_new.a[a] : fluid_new.b[a - 6]) + ro + xtab[1 + k];
+        cp_async8(sb + (MS_FL + a) * W + 1 + k, src);
+      }
+      for (int i = tid; i < 3 * W; i += NT) {
+        const int c = i / W, k = i - c * W;
+        cp_async8(sb + (MS_BY + c) * W + k, fields_old.f[BY1 + c] + ro + xtab[k]);
+      }
+      for (int i = tid; i < 6 * TX; i += NT) {
+        const int a = i / TX, k = i - a * TX;
+        const double* base = (a < 3) ? fields_old.f[AZ1 + a] : fields_old.f[EX1 + a - 3];
+        cp_async8(sb + (MS_AZ + a) * W + 1 + k, base + ro + xtab[1 + k]);
+      }
+      for (int i = tid; i < 3 * (TX + 1); i += NT) {
+        const int c = i / (TX + 1), k = i - c * (TX + 1);
+        cp_async8(sb + (MS_EZ + c) * W + 1 + k, fields_old.f[EZ1 + c] + ro + xtab[1 + k]);
+      }
+    };
+
+    // Rows q-1 and q are read in the same iteration, so NST-2 rows are in
+    // flight and the refill goes to the stage of row q-2.
+    const int q_first = zs - 1, q_last = ze;
 #pragma unroll
-      for (int a = 0; a < 3; ++a) az[a] = s_az[a][zz][xx];
-      if (!p.freeze_az1) az[0] = az[0] - dt * s_ez[0][zz][xx];
-      az[1] = az[1] - dt * s_ez[1][zz][xx];
-      az[2] = az[2] - dt * s_ez[2][zz][xx];
-      const double e1 = s_ex[0][zz][xx], e2 = s_ex[1][zz][xx], e3 = s_ex[2][zz][xx];
-      const double k[3] = {az[1] * e3 - az[2] * e2, az[2] * e1 - az[0] * e3, az[0] * e2 - az[1] * e1};
+    for (int k = 0; k < NST - 2; ++k) {
+      if (q_first + k <= q_last) issue_row(q_first + k, k);
+      cp_async_commit();
+    }
+
+    for (int q = q_first, it = 0; q <= q_last; ++q, ++it) {
+      cp_async_wait<NST - 3>();
+      __syncthreads();  // row q staged by every thread; row q-2's stage is free
+      {
+        const int qn = q + NST - 2;
+        if (qn <= q_last) issue_row(qn, (it + NST - 2) % NST);
+        cp_async_commit();
+      }
+      const double* sb = stage + (size_t)(it % NST) * MS_SIZE * W;                 // row q
+      const double* sp = stage + (size_t)((it + NST - 1) % NST) * MS_SIZE * W;     // row q-1
+      const int rq = q & 1, rp = (q - 1) & 1;
+
+      // ---- 1: per-cell velocities of row q (YM_Physics.cu:22-25, 38-41)
+      for (int i = tid; i < 2 * (TX + 1); i += NT) {
+        const int b = i / (TX + 1), k = 1 + (i - b * (TX + 1));
+        const double* fl = sb + (size_t)(MS_FL + 6 * b) * W;
+        const double n = fmax(fl[FN * W + k], 1e-10);
+        wk[(MW_V + rq * 4 + b * 2 + 0) * W + k] = fl[FPX * W + k] / n;
+        wk[(MW_V + rq * 4 + b * 2 + 1) * W + k] = fl[FPZ * W + k] / n;
+      }
+      __syncthreads();
+
+      // ---- 2a: Ampère for Ex on row q, columns [x0, x0+TX) (threads [0, TX))
+      if (tid < TX) {
+        const int k = 1 + tid;
+        double nq[2][3], vxr[2];
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const double dex = (s_ex[a][zz + 1][xx] - s_ex[a][zz][xx]) / p.dz;
-        const double dez = (s_ez[a][zz][xx + 1] - s_ez[a][zz][xx]) / p.dx;
-        const double byo = s_by[a][zz + 1][xx + 1];
-        out.f[BY1 + a][gi] = byo - dt * (dex - dez - al * k[a]);
-        out.f[EX1 + a][gi] = s_ex[a][zz][xx];
-        out.f[EZ1 + a][gi] = s_ez[a][zz][xx];
-        out.f[AZ1 + a][gi] = az[a];
+        for (int b = 0; b < 2; ++b) {
+          const double* fl = sb + (size_t)(MS_FL + 6 * b) * W;
+          const double n0 = fl[FN * W + k], n1 = fl[FN * W + k + 1];
+          vxr[b] = 0.5 * (wk[(MW_V + rq * 4 + b * 2) * W + k] + wk[(MW_V + rq * 4 + b * 2) * W + k + 1]);
+#pragma unroll
+          for (int a = 0; a < 3; ++a) nq[b][a] = 0.5 * (n0 * fl[(FQ1 + a) * W + k] + n1 * fl[(FQ1 + a) * W + k + 1]);
+        }
+        const double by1 = sb[(MS_BY + 0) * W + k], by2 = sb[(MS_BY + 1) * W + k], by3 = sb[(MS_BY + 2) * W + k];
+        const double d1 = (by1 - sp[(MS_BY + 0) * W + k]) / p.dz;
+        const double d2 = (by2 - sp[(MS_BY + 1) * W + k]) / p.dz;
+        const double d3 = (by3 - sp[(MS_BY + 2) * W + k]) / p.dz;
+        const double a1 = sb[(MS_AZ + 0) * W + k], a2 = sb[(MS_AZ + 1) * W + k], a3 = sb[(MS_AZ + 2) * W + k];
+        const double kx[3] = {a2 * by3 - a3 * by2, a3 * by1 - a1 * by3, a1 * by2 - a2 * by1};
+        const double dz3[3] = {d1, d2, d3};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const double jx = -(nq[0][a] * vxr[0] + nq[1][a] * vxr[1]);
+          wk[(MW_EX + rq * 3 + a) * W + k] = sb[(MS_EX + a) * W + k] + dt * (c2 * (-dz3[a] - al * kx[a]) - jx / e0);
+        }
+      } else {
+        // ---- 2b: Ampère for Ez on row q-1, columns [x0, x0+TX] (threads [TX, 2TX) + one extra)
+        for (int i = tid - TX; i < TX + 1; i += NT - TX) {
+          const int k = 1 + i;
+          double nqz[2][3], vzt[2];
+#pragma unroll
+          for (int b = 0; b < 2; ++b) {
+            const double* f0 = sp + (size_t)(MS_FL + 6 * b) * W;
+            const double* f1 = sb + (size_t)(MS_FL + 6 * b) * W;
+            const double n0 = f0[FN * W + k], n1 = f1[FN * W + k];
+            vzt[b] = 0.5 * (wk[(MW_V + rp * 4 + b * 2 + 1) * W + k] + wk[(MW_V + rq * 4 + b * 2 + 1) * W + k]);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) nqz[b][a] = 0.5 * (n0 * f0[(FQ1 + a) * W + k] + n1 * f1[(FQ1 + a) * W + k]);
+          }
+          const int gx = xtab[k];
+          const bool wz = wall && (gx == 0 || gx == nx - 1);  // YM_Fluid.cu:25-29
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const double jz = -(nqz[0][a] * vzt[0] + nqz[1][a] * vzt[1]);
+            const double by = sp[(MS_BY + a) * W + k];
+            const double dbx = (by - sp[(MS_BY + a) * W + k - 1]) / p.dx;
+            const double ez0 = wz ? 0.0 : sp[(MS_EZ + a) * W + k];
+            wk[(MW_EZ + a) * W + k] = ez0 + dt * (c2 * dbx - jz / e0);
+          }
+        }
+      }
+      __syncthreads();
+      // At a wall the right neighbour of the last column is the column itself
+      // (YM_Physics.cu:127): its Ez is that column's new Ez.
+      if (wall && x0 + TX >= nx) {
+        if (tid < 3) {
+          const int kl = 1 + (nx - 1 - x0);
+          wk[(MW_EZ + tid) * W + kl + 1] = wk[(MW_EZ + tid) * W + kl];
+        }
+        __syncthreads();
+      }
+
+      // ---- 3: potential and Faraday on row q-1 (threads [0, TX))
+      const int o = q - 1;
+      if (tid < TX && o >= zs && o < ze && x0 + tid < nx) {
+        const int k = 1 + tid;
+        const size_t gi = idx2(x0 + tid, o, nx);
+        double az[3], ex[3], ez[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          az[a] = sp[(MS_AZ + a) * W + k];
+          ex[a] = wk[(MW_EX + rp * 3 + a) * W + k];
+          ez[a] = wk[(MW_EZ + a) * W + k];
+        }
+        if (!p.freeze_az1) az[0] = az[0] - dt * ez[0];
+        az[1] = az[1] - dt * ez[1];
+        az[2] = az[2] - dt * ez[2];
+        const double kk[3] = {az[1] * ex[2] - az[2] * ex[1], az[2] * ex[0] - az[0] * ex[2],
+                              az[0] * ex[1] - az[1] * ex[0]};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const double dex = (wk[(MW_EX + rq * 3 + a) * W + k] - ex[a]) / p.dz;
+          const double dez = (wk[(MW_EZ + a) * W + k + 1] - ez[a]) / p.dx;
+          out.f[BY1 + a][gi] = sp[(MS_BY + a) * W + k] - dt * (dex - dez - al * kk[a]);
+          out.f[EX1 + a][gi] = ex[a];
+          out.f[EZ1 + a][gi] = ez[a];
+          out.f[AZ1 + a][gi] = az[a];
+        }
       }
     }
+    cp_async_wait<0>();
   }
 }
 
+cudaError_t prepare_maxwell() {
+  return cudaFuncSetAttribute(maxwell_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)maxwell_smem_bytes());
+}
+
+int maxwell_ctas_per_sm() {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, maxwell_fused_kernel, MX_NT, maxwell_smem_bytes());
+  return n;
+}
+
 cudaError_t launch_maxwell(const State& fluid_new, const State& fields_old, const State& out, const StepParams& p,
-                           cudaStream_t s) {
-  dim3 grid((p.nx + MX_TX - 1) / MX_TX, (p.nz + MX_TZ - 1) / MX_TZ);
-  maxwell_fused_kernel<<<grid, MX_TX * MX_TZ, 0, s>>>(fluid_new, fields_old, out, p);
+                           int seg_len, int grid_ctas, cudaStream_t s) {
+  MxSched sc;
+  sc.nstrips = (p.nx + MX_TX - 1) / MX_TX;
+  sc.seg_len = seg_len;
+  sc.nitems = sc.nstrips * ((p.nz + seg_len - 1) / seg_len);
+  const int grid = std::min(sc.nitems, grid_ctas);
+  maxwell_fused_kernel<<<grid, MX_NT, maxwell_smem_bytes(), s>>>(fluid_new, fields_old, out, p, sc);
   return cudaGetLastError();
 }
 

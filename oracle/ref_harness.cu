@@ -252,9 +252,14 @@ int ymref_create(const ymkh_grid* grid, const ymkh_params* p, int raise_zmean_sm
   g.h_ebuf.assign((size_t)g.nx * g.nz, 0.0);
   for (void* a : g.allocs)
     if (!a) { snprintf(g_err, sizeof g_err, "cudaMalloc failed"); ymref_destroy(); return YMKH_ENOMEM; }
-  if (g.raise_smem) {
-    RCHK(cudaFuncSetAttribute(kernel_ym_subtract_zmean, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)(15 * g.nz * sizeof(double))));
+  // Raise the z-mean kernel's shared-memory limit where the device allows it
+  // (NZ = 512, 1024); beyond that the reference's launch fails as it does
+  // in the stock loop, and this harness reports the failed launch.
+  const int zsm = (int)(15 * g.nz * sizeof(double));
+  int optin = 0;
+  RCHK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, 0));
+  if (g.raise_smem && q.suppress_kz0 && zsm > 48 * 1024 && zsm <= optin) {
+    RCHK(cudaFuncSetAttribute(kernel_ym_subtract_zmean, cudaFuncAttributeMaxDynamicSharedMemorySize, zsm));
   }
   g.live = true;
   RCHK(cudaDeviceSynchronize());
