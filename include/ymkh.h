@@ -171,6 +171,12 @@ int ymkh_energy_async(ymkh_ctx* ctx, double* dev_out, void* stream);
  * out[1] = the same for the conjugate signal (Az2 - i Az3). */
 int ymkh_mode_amp(ymkh_ctx* ctx, int k, double* host_out2, void* stream);
 
+/* Reports (and clears) a failure of the bounded waits inside the kernels
+ * (a staged row that never arrived): YMKH_ECUDA if one timed out since the
+ * last check.  Synchronises `stream`; ymkh_energy calls it.  No reference
+ * counterpart. */
+int ymkh_check(ymkh_ctx* ctx, void* stream);
+
 /* Frees the context (not the bound state). */
 int ymkh_destroy(ymkh_ctx* ctx);
 

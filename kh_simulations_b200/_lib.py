@@ -81,6 +81,7 @@ _SIGS = {
     "ymkh_energy_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "ymkh_mode_amp": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_void_p]),
     "ymkh_destroy": (C.c_int, [C.c_void_p]),
+    "ymkh_check": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ymkh_twiddles": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "ymkh_launch_count": (C.c_longlong, []),
     "ymkh_stage_times": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_float), C.c_int]),

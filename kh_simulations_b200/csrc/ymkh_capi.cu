@@ -74,6 +74,8 @@ struct ymkh_ctx {
   int fct_tx = 64, fct_seg = 16, fct_grid = 296;  // FCT threads per beam, segment rows, persistent CTAs
   int mx_seg = 16, mx_grid = 148;                   // Maxwell segment rows, persistent CTAs
   int sms = 148;
+  bool aligned16 = false;   // every bound array 16-byte aligned: TMA bulk row copies allowed
+  unsigned* derr = nullptr; // device error word of the bounded in-kernel waits
   // CUDA graphs of `graph_steps` steps, one per starting buffer
   int graph_steps = 4;
   cudaGraphExec_t gexec[2]{nullptr, nullptr};
@@ -170,11 +172,12 @@ void choose_launch_shape(ymkh_ctx* c) {
   c->fct_tx = c->nx >= 128 ? 64 : 32;
   const int fct_per_sm = std::max(1, fct_ctas_per_sm(c->fct_tx));
   c->fct_grid = c->sms * fct_per_sm;
-  const int fstrips = (c->nx + (c->fct_tx - 4) - 1) / (c->fct_tx - 4);
+  const int fstrips = (c->nx + (c->fct_tx - 6) - 1) / (c->fct_tx - 6);
   c->fct_seg = pick_segment(c->nz, fstrips, c->fct_grid);
   const int mx_per_sm = std::max(1, maxwell_ctas_per_sm());
   c->mx_grid = c->sms * mx_per_sm;
-  c->mx_seg = pick_segment(c->nz, (c->nx + 127) / 128, c->mx_grid);
+  const int mw = maxwell_strip_width();
+  c->mx_seg = pick_segment(c->nz, (c->nx + mw - 1) / mw, c->mx_grid);
 }
 
 ArrayList list21(const State& s) {
@@ -204,9 +207,9 @@ int step_once(ymkh_ctx* c, cudaStream_t s) {
   const State& in = c->buf[c->cur];
   const State& out = c->buf[1 - c->cur];
   mark(c, ST_FCT, s);
-  CK(launch_fct(in, out, c->sp, c->fct_tx, c->fct_seg, c->fct_grid, s), "fct_fused_kernel");
+  CK(launch_fct(in, out, c->sp, c->fct_tx, c->fct_seg, c->fct_grid, c->aligned16, c->derr, s), "fct_fused_kernel");
   mark(c, ST_MAXWELL, s);
-  CK(launch_maxwell(out, in, out, c->sp, c->mx_seg, c->mx_grid, s), "maxwell_fused_kernel");
+  CK(launch_maxwell(out, in, out, c->sp, c->mx_seg, c->mx_grid, c->aligned16, c->derr, s), "maxwell_fused_kernel");
   mark(c, ST_POINTWISE, s);
   g_launches += 2;
   if (c->prm.xi_sponge > 0.0) { CK(launch_sponge_xicut(list12(out), c->sp, 0, s), "sponge"); g_launches++; }
@@ -307,7 +310,8 @@ int ymkh_create(const ymkh_grid* grid, const ymkh_params* params, ymkh_ctx** out
   const int np = energy_nparts(c->N);
   if (cudaMalloc(&c->epart, (size_t)2 * np * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->edev, 4 * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&c->mcol, (size_t)2 * c->nx * sizeof(double)) != cudaSuccess) {
+      cudaMalloc(&c->mcol, (size_t)2 * c->nx * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->derr, sizeof(unsigned)) != cudaSuccess || cudaMemset(c->derr, 0, sizeof(unsigned)) != cudaSuccess) {
     ymkh_destroy(c);
     return set_err(YMKH_ENOMEM, "cudaMalloc diagnostics");
   }
@@ -327,6 +331,13 @@ static State make_state(double* const f[12], double* const a[6], double* const b
   for (int i = 0; i < 12; ++i) s.f[i] = f[i];
   for (int i = 0; i < 6; ++i) { s.a[i] = a[i]; s.b[i] = b[i]; }
   return s;
+}
+
+static bool aligned16(const State& s) {
+  for (int i = 0; i < 12; ++i) if (reinterpret_cast<uintptr_t>(s.f[i]) % 16) return false;
+  for (int i = 0; i < 6; ++i)
+    if (reinterpret_cast<uintptr_t>(s.a[i]) % 16 || reinterpret_cast<uintptr_t>(s.b[i]) % 16) return false;
+  return true;
 }
 
 static bool state_ok(const State& s) {
@@ -354,6 +365,7 @@ int ymkh_bind_state(ymkh_ctx* c, double* const fields[YMKH_NFIELDS], double* con
   c->dual = false;
   c->cur = 0;
   c->bound = true;
+  c->aligned16 = aligned16(c->buf[0]) && aligned16(c->buf[1]);
   return 0;
 }
 
@@ -371,6 +383,21 @@ int ymkh_bind_state2(ymkh_ctx* c, double* const* state0, double* const* state1) 
   c->dual = true;
   c->cur = 0;
   c->bound = true;
+  c->aligned16 = aligned16(s0) && aligned16(s1);
+  return 0;
+}
+
+// Reads (and clears) the device error word set by in-kernel waits that ran
+// out of polls; synchronises the stream.
+int ymkh_check(ymkh_ctx* c, void* stream) {
+  if (!c) return set_err(YMKH_EINVAL, "null context");
+  unsigned h = 0;
+  CK(cudaMemcpyAsync(&h, c->derr, sizeof h, cudaMemcpyDeviceToHost, (cudaStream_t)stream), "error word D2H");
+  CK(cudaStreamSynchronize((cudaStream_t)stream), "error word sync");
+  if (h) {
+    cudaMemsetAsync(c->derr, 0, sizeof(unsigned), (cudaStream_t)stream);
+    return set_err(YMKH_ECUDA, "a bounded in-kernel wait timed out (error word %u); results of that step are invalid", h);
+  }
   return 0;
 }
 
@@ -506,8 +533,7 @@ int ymkh_energy(ymkh_ctx* c, double* host_out, void* stream) {
   int rc = ymkh_energy_async(c, c ? c->edev : nullptr, stream);
   if (rc) return rc;
   CK(cudaMemcpyAsync(host_out, c->edev, sizeof(double), cudaMemcpyDeviceToHost, (cudaStream_t)stream), "energy D2H");
-  CK(cudaStreamSynchronize((cudaStream_t)stream), "energy sync");
-  return 0;
+  return ymkh_check(c, stream);
 }
 
 int ymkh_mode_amp(ymkh_ctx* c, int k, double* host_out2, void* stream) {
@@ -530,6 +556,7 @@ int ymkh_destroy(ymkh_ctx* c) {
   if (c->epart) cudaFree(c->epart);
   if (c->edev) cudaFree(c->edev);
   if (c->mcol) cudaFree(c->mcol);
+  if (c->derr) cudaFree(c->derr);
   delete c;
   return 0;
 }

@@ -111,11 +111,12 @@ struct InitArgs {
 cudaError_t prepare_fct(int tb);
 int fct_ctas_per_sm(int tb);
 cudaError_t launch_fct(const State& in, const State& out, const StepParams& p, int tb, int seg_len, int grid_ctas,
-                       cudaStream_t s);
+                       bool allow_bulk, unsigned* err, cudaStream_t s);
 cudaError_t prepare_maxwell();
 int maxwell_ctas_per_sm();
+int maxwell_strip_width();
 cudaError_t launch_maxwell(const State& fluid_new, const State& fields_old, const State& out, const StepParams& p,
-                           int seg_len, int grid_ctas, cudaStream_t s);
+                           int seg_len, int grid_ctas, bool allow_bulk, unsigned* err, cudaStream_t s);
 cudaError_t launch_sponge_xicut(const ArrayList& a12, const StepParams& p, int cut, cudaStream_t s);
 cudaError_t prepare_column(int nz);
 cudaError_t launch_zmean(const ArrayList& a15, int nx, int nz, cudaStream_t s);
@@ -129,5 +130,58 @@ int energy_nparts(size_t N);
 cudaError_t launch_mode_amp(const double* az2, const double* az3, int nx, int nz, int k, double* colbuf, double* out,
                             cudaStream_t s);
 cudaError_t launch_init(const State& st, const InitArgs& a, cudaStream_t s);
+
+}  // namespace ymkh
+
+namespace ymkh {
+
+// ---- TMA bulk copies (cp.async.bulk, global -> shared, mbarrier completion)
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
+  unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+// Spin on the phase with a bounded number of polls; on timeout the error
+// word is set and the caller carries on (the host reports it), so a lost
+// completion can never hang the GPU.
+__device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned phase, unsigned* err) {
+  unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  for (long it = 0; it < (1L << 26); ++it) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(phase)
+        : "memory");
+    if (done) return;
+  }
+  if (err) atomicOr(err, 1u);
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(d),
+               "l"(src), "r"(bytes), "r"(b)
+               : "memory");
+}
+// count doubles of a periodic row starting at shear index xs (which may be
+// negative or past the end), split at the wrap.  Requires nx even, xs even,
+// count even and count <= nx so every piece is 16-byte aligned and sized.
+__device__ __forceinline__ void bulk_row_periodic(double* dst, const double* row, int xs, int count, int nx,
+                                                  uint64_t* bar) {
+  int x = xs % nx;
+  if (x < 0) x += nx;
+  int done = 0;
+  while (done < count) {
+    const int len = min(count - done, nx - x);
+    bulk_g2s(dst + done, row + x, (unsigned)len * 8u, bar);
+    done += len;
+    x = 0;
+  }
+}
 
 }  // namespace ymkh

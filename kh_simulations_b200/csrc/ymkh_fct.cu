@@ -12,12 +12,16 @@
 // start-of-step state, which is what they are a function of.
 //
 // Layout: work items are (x-strip, z-segment) pairs, handed to persistent
-// CTAs round-robin.  A strip emits TB-4 columns [x0, x0+TB-4); thread t of a
-// beam owns x-sweep position x0-2+t, so every x-sweep phase is exactly one
-// position per thread.  Threads [0,TB) handle beam A, [TB,2TB) beam B; the
-// beams synchronise only through their own named barriers.  Row data (12
-// fluid arrays plus the field rows the sources need) is staged in shared
-// memory with cp.async NST-1 rows ahead.  For each row the x-sweep
+// CTAs round-robin.  A strip emits TB-6 columns; thread t of a beam owns
+// stage position t+1 (shear index x0-3+t), and every x-sweep phase is at
+// most one position or interface per thread: interface quantities (eps, nu,
+// mu, low-order fluxes) are formed once per interface.  Threads [0,TB)
+// handle beam A, [TB,2TB) beam B; the beams synchronise only through their
+// own named barriers.  Row data (12 fluid arrays plus the field rows the
+// sources need) is staged in shared memory NST-1 rows ahead: one thread
+// issues TMA bulk copies (cp.async.bulk, split at the periodic wrap) that
+// complete on a per-stage mbarrier; wall boundaries use per-element cp.async
+// with clamped indices.  For each row the x-sweep
 // (FCT_Sweeps.cu:88-162) runs across the strip in shared memory; its result
 // for the thread's own column feeds a register pipeline that performs the
 // z-sweep along the stream, emitting row r-3 once row r arrives (halo 3,
@@ -32,13 +36,13 @@ namespace ymkh {
 
 namespace {
 
-// Offsets (in units of W doubles) inside one stage buffer; stage position
-// sp holds shear index x = x0 - 4 + sp.
-constexpr int ST_FL = 0;     // fluid: (beam*6 + var), sp in [1, TB+3)
-constexpr int ST_EX = 12;    // Ex1..3 row zr,         sp in [1, TB+2)
-constexpr int ST_BY = 15;    // By1..3 row zr,         sp in [1, TB+2)
-constexpr int ST_BYM = 18;   // By1..3 row zm,         sp in [1, TB+2)
-constexpr int ST_EZ = 21;    // Ez1..3 row zr,         sp in [4, TB)
+// Stage layout (units of W doubles); stage position sp holds shear index
+// x = x0 - 4 + sp, sp in [0, W) with W = TB + 2.
+constexpr int ST_FL = 0;     // fluid: (beam*6 + var)
+constexpr int ST_EX = 12;    // Ex1..3 row zr
+constexpr int ST_BY = 15;    // By1..3 row zr
+constexpr int ST_BYM = 18;   // By1..3 row zm
+constexpr int ST_EZ = 21;    // Ez1..3 row zr
 constexpr int ST_EZM = 24;   // Ez1..3 row zm
 constexpr int ST_AZ = 27;    // Az1..3 row zr
 constexpr int ST_AZM = 30;   // Az1..3 row zm
@@ -46,49 +50,74 @@ constexpr int ST_NZP = 33;   // n (beam A, B) row zp (warm_T only)
 constexpr int ST_NZM = 35;   // n (beam A, B) row zm (warm_T only)
 constexpr int ST_SIZE = 37;
 
-// Per-beam work arrays (units of W), indexed by stage position.
-constexpr int WB_U = 0, WB_LOR = 1, WB_LNR = 7, WB_FLIM = 13, WB_SIZE = 19;
+// Per-beam work arrays (units of W), by stage position / interface index
+// (interface j+1/2 stored at j).  Fluxes F, D are dead after phase B, so the
+// limited fluxes reuse their space.
+constexpr int WB_MU = 0, WB_F = 1, WB_D = 7, WB_FLIM = 1, WB_LOR = 13, WB_LNR = 19, WB_SIZE = 25;
 
 __device__ __forceinline__ void beam_bar(int beam, int nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(beam + 1), "r"(nthreads) : "memory");
+}
+
+// apply_fct_limiter (FCT_DeviceMath.cuh:108-125) with the products by
+// copysign(1, d0) written as sign selections, which give the same values.
+__device__ __forceinline__ double fct_limit_sel(double f, double dm1, double d0, double dp1) {
+  const bool neg = signbit(d0);
+  const double term = neg ? -dm1 : dm1;
+  const double terp = neg ? -dp1 : dp1;
+  const double r = fmax(0.0, fmin(term, fmin(fabs(f), terp)));
+  return neg ? -r : r;
 }
 
 }  // namespace
 
 template <int TB>
 constexpr size_t fct_smem_bytes(int nst) {
-  return (size_t)(TB + 4) * sizeof(double) * (nst * ST_SIZE + 2 * WB_SIZE) + (size_t)(TB + 4) * sizeof(int);
+  return (size_t)(TB + 2) * sizeof(double) * (nst * ST_SIZE + 2 * WB_SIZE) + (size_t)(TB + 2) * sizeof(int) +
+         (size_t)8 * nst + 16;
 }
 
 struct FctSched {
-  int nstrips;   // strips of TB-4 output columns
+  int nstrips;   // strips of TB-6 output columns
   int seg_len;   // rows per z-segment
   int nitems;    // nstrips * nsegments
+  int bulk;      // 1: TMA bulk row copies (periodic x, even NX >= TB+2)
+  unsigned* err; // device error word (bounded waits that ran out)
 };
 
 template <int TB, int NST>
 __global__ void __launch_bounds__(2 * TB)
     fct_fused_kernel(const __grid_constant__ State st, const __grid_constant__ State out,
                      const __grid_constant__ StepParams p, const FctSched sc) {
-  constexpr int W = TB + 4;
+  constexpr int W = TB + 2;
   constexpr int NT = 2 * TB;
-  constexpr int TO = TB - 4;  // output columns per strip
+  constexpr int TO = TB - 6;  // output columns per strip
   extern __shared__ __align__(16) double smem[];
   double* const stage = smem;
   double* const wk = smem + (size_t)NST * ST_SIZE * W;
   int* const xtab = reinterpret_cast<int*>(wk + (size_t)2 * WB_SIZE * W);
+  uint64_t* const bars = reinterpret_cast<uint64_t*>(
+      (reinterpret_cast<uintptr_t>(xtab + W) + 15) & ~static_cast<uintptr_t>(15));
 
   const int nx = p.nx, nz = p.nz;
   const int tid = threadIdx.x;
   const int beam = tid / TB;
   const int t = tid - beam * TB;
-  const int sp = t + 2;  // stage position of this thread's x-sweep position
+  const int sp = t + 1;  // this thread's stage position
   const bool warm = p.warm_T > 0.0;
   const bool wall = !p.periodic_x;
+  const bool bulk = sc.bulk != 0;
   const double dt = p.dt;
   const double dtdx = p.dt / p.dx;
   const double dtdz = p.dt / p.dz;
   double* const wb = wk + (size_t)beam * WB_SIZE * W;
+
+  if (bulk && tid == 0) {
+    for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  unsigned issued = 0, consumed = 0;  // rows issued / consumed by this CTA (all items)
 
   for (int item = blockIdx.x; item < sc.nitems; item += gridDim.x) {
     const int strip = item % sc.nstrips;
@@ -97,154 +126,180 @@ __global__ void __launch_bounds__(2 * TB)
     const int ze = min(nz, zs + sc.seg_len);
 
     __syncthreads();  // previous item fully consumed
-    for (int i = tid; i < W; i += NT) xtab[i] = xmap(x0 - 4 + i, nx, p.periodic_x);
+    if (!bulk)
+      for (int i = tid; i < W; i += NT) xtab[i] = xmap(x0 - 4 + i, nx, p.periodic_x);
     __syncthreads();
 
-    auto issue_row = [&](int r, int s) {
+    // Stage one row (clamped z index).  Bulk path: thread 0 arms the stage's
+    // mbarrier and issues whole-row copies; element path: every thread
+    // issues 8-byte cp.async with clamped shear indices.
+    auto issue_row = [&](int r) {
+      const int s = (int)(issued % NST);
       double* sb = stage + (size_t)s * ST_SIZE * W;
       const int zr = zclamp(r, nz);
       const int zm = (zr == 0) ? nz - 1 : zr - 1;
       const int zp = (zr == nz - 1) ? 0 : zr + 1;
       const size_t ro = (size_t)zr * nx, rom = (size_t)zm * nx, rop = (size_t)zp * nx;
-      for (int i = tid; i < 12 * (TB + 2); i += NT) {
-        const int a = i / (TB + 2), q = i - a * (TB + 2);
-        const double* src = (a < 6 ? st.a[a] : st.b[a - 6]) + ro + xtab[1 + q];
-        cp_async8(sb + (ST_FL + a) * W + 1 + q, src);
-      }
-      for (int i = tid; i < 9 * (TB + 1); i += NT) {
-        const int a = i / (TB + 1), q = i - a * (TB + 1);
-        const int c = a % 3;
-        const double* base = (a < 3) ? st.f[EX1 + c] : st.f[BY1 + c];
-        cp_async8(sb + (ST_EX + a) * W + 1 + q, base + (a < 6 ? ro : rom) + xtab[1 + q]);
-      }
-      for (int i = tid; i < 12 * TO; i += NT) {
-        const int a = i / TO, q = i - a * TO;
-        const int c = a % 3, kind = a / 3;
-        const double* base = (kind < 2) ? st.f[EZ1 + c] : st.f[AZ1 + c];
-        cp_async8(sb + (ST_EZ + a) * W + 4 + q, base + ((kind & 1) ? rom : ro) + xtab[4 + q]);
-      }
-      if (warm) {
-        for (int i = tid; i < 4 * TO; i += NT) {
-          const int a = i / TO, q = i - a * TO;
-          const double* base = (a & 1) ? st.b[FN] : st.a[FN];
-          cp_async8(sb + (ST_NZP + a) * W + 4 + q, base + ((a >> 1) ? rom : rop) + xtab[4 + q]);
+      if (bulk) {
+        if (tid == 0) {
+          const int narr = 33 + (warm ? 4 : 0);
+          mbar_expect_tx(&bars[s], (unsigned)(narr * W * 8));
+          const int xs = x0 - 4;
+          for (int a = 0; a < 12; ++a)
+            bulk_row_periodic(sb + (ST_FL + a) * W, (a < 6 ? st.a[a] : st.b[a - 6]) + ro, xs, W, nx, &bars[s]);
+          for (int c = 0; c < 3; ++c) {
+            bulk_row_periodic(sb + (ST_EX + c) * W, st.f[EX1 + c] + ro, xs, W, nx, &bars[s]);
+            bulk_row_periodic(sb + (ST_BY + c) * W, st.f[BY1 + c] + ro, xs, W, nx, &bars[s]);
+            bulk_row_periodic(sb + (ST_BYM + c) * W, st.f[BY1 + c] + rom, xs, W, nx, &bars[s]);
+            bulk_row_periodic(sb + (ST_EZ + c) * W, st.f[EZ1 + c] + ro, xs, W, nx, &bars[s]);
+            bulk_row_periodic(sb + (ST_EZM + c) * W, st.f[EZ1 + c] + rom, xs, W, nx, &bars[s]);
+            bulk_row_periodic(sb + (ST_AZ + c) * W, st.f[AZ1 + c] + ro, xs, W, nx, &bars[s]);
+            bulk_row_periodic(sb + (ST_AZM + c) * W, st.f[AZ1 + c] + rom, xs, W, nx, &bars[s]);
+          }
+          if (warm) {
+            bulk_row_periodic(sb + (ST_NZP + 0) * W, st.a[FN] + rop, xs, W, nx, &bars[s]);
+            bulk_row_periodic(sb + (ST_NZP + 1) * W, st.b[FN] + rop, xs, W, nx, &bars[s]);
+            bulk_row_periodic(sb + (ST_NZM + 0) * W, st.a[FN] + rom, xs, W, nx, &bars[s]);
+            bulk_row_periodic(sb + (ST_NZM + 1) * W, st.b[FN] + rom, xs, W, nx, &bars[s]);
+          }
         }
+      } else {
+        for (int i = tid; i < 12 * (W - 1); i += NT) {
+          const int a = i / (W - 1), q = 1 + (i - a * (W - 1));
+          cp_async8(sb + (ST_FL + a) * W + q, (a < 6 ? st.a[a] : st.b[a - 6]) + ro + xtab[q]);
+        }
+        for (int i = tid; i < 21 * (W - 1); i += NT) {
+          const int a = i / (W - 1), q = 1 + (i - a * (W - 1));
+          const int kind = a / 3, c = a - kind * 3;  // EX, BY, BYM, EZ, EZM, AZ, AZM
+          const double* base = (kind == 0) ? st.f[EX1 + c]
+                               : (kind <= 2) ? st.f[BY1 + c]
+                               : (kind <= 4) ? st.f[EZ1 + c]
+                                             : st.f[AZ1 + c];
+          const size_t off = (kind == 2 || kind == 4 || kind == 6) ? rom : ro;
+          cp_async8(sb + (ST_EX + a) * W + q, base + off + xtab[q]);
+        }
+        if (warm) {
+          for (int i = tid; i < 4 * (W - 1); i += NT) {
+            const int a = i / (W - 1), q = 1 + (i - a * (W - 1));
+            const double* base = (a & 1) ? st.b[FN] : st.a[FN];
+            cp_async8(sb + (ST_NZP + a) * W + q, base + ((a >> 1) ? rom : rop) + xtab[q]);
+          }
+        }
+        cp_async_commit();
       }
+      ++issued;
     };
 
     const int r_first = zs - 3, r_last = ze + 2;
-#pragma unroll
-    for (int k = 0; k < NST - 1; ++k) {
-      if (r_first + k <= r_last) issue_row(r_first + k, k);
-      cp_async_commit();
-    }
+    for (int k = 0; k < NST - 1; ++k)
+      if (r_first + k <= r_last) issue_row(r_first + k);
+      else if (!bulk) cp_async_commit();
 
     double V1[6], f1[6], d1[6], L2[6], N4[6], N3[6], N2[6], A2[6], F3[6], S1[6];
 #pragma unroll
     for (int k = 0; k < 6; ++k) V1[k] = f1[k] = d1[k] = L2[k] = N4[k] = N3[k] = N2[k] = A2[k] = F3[k] = S1[k] = 0.0;
     double U1 = 0.0, mu1 = 0.0;
-    const int x_own = x0 - 2 + t;
-    const bool owner = (t >= 2) && (t < TB - 2) && (x_own < nx);
+    const int x_own = x0 - 4 + sp;
+    const bool zthread = (t >= 3) && (t < TB - 3);          // owns an output column
+    const bool owner = zthread && (x_own < nx);
 
-    for (int r = r_first, it = 0; r <= r_last; ++r, ++it) {
-      cp_async_wait<NST - 2>();
-      __syncthreads();  // row r staged by every thread; row r-1's stage is free
-      {
-        const int rn = r + NST - 1;
-        if (rn <= r_last) issue_row(rn, (it + NST - 1) % NST);
-        cp_async_commit();
-      }
-      const double* sb = stage + (size_t)(it % NST) * ST_SIZE * W;
+    for (int r = r_first; r <= r_last; ++r) {
+      const int s = (int)(consumed % NST);
+      if (bulk)
+        mbar_wait(&bars[s], (consumed / NST) & 1u, sc.err);
+      else
+        cp_async_wait<NST - 2>();
+      __syncthreads();  // row r staged for everyone; the previous row's stage is free
+      ++consumed;
+      if (r + NST - 1 <= r_last) issue_row(r + NST - 1);
+      else if (!bulk) cp_async_commit();
+      const double* sb = stage + (size_t)s * ST_SIZE * W;
       const double* fl = sb + (size_t)(ST_FL + beam * 6) * W;
 
-      // ---- A: velocities (YM_Fluid.cu:3-11) at sp (and the two edge
-      // positions), px source (YM_Fluid.cu:43-66, 71-80) at sp.
-      double vz_own;
+      // ---- A: velocities at sp, sp+1 (YM_Fluid.cu:3-11); interface sp+1/2:
+      // eps, nu, mu and the low-order fluxes (FCT_Sweeps.cu:88-98); px
+      // source at sp (YM_Fluid.cu:43-66, 71-80).
+      double vz_own = 0.0, ux_own = 0.0, sx = 0.0;
       {
-        const double ns = fmax(fl[FN * W + sp], 0.05);
-        wb[WB_U * W + sp] = fl[FPX * W + sp] / ns;
-        vz_own = fl[FPZ * W + sp] / ns;
-        if (t == 0 || t == TB - 1) {
-          const int e = (t == 0) ? 1 : TB + 2;
-          const double ne = fmax(fl[FN * W + e], 0.05);
-          wb[WB_U * W + e] = fl[FPX * W + e] / ne;
-        }
-      }
-      double sx;
-      {
-        int ps = sp;  // at a wall the clamped ghost cells carry the edge cell's source
-        if (wall) {
-          const int xg = x0 - 4 + sp;
-          ps = (xg < 0 ? 0 : (xg >= nx ? nx - 1 : xg)) - (x0 - 4);
-        }
-        const double vz = (ps == sp) ? vz_own : fl[FPZ * W + ps] / fmax(fl[FN * W + ps], 0.05);
-        double acc;
-        {
-          const double ex = 0.5 * (sb[(ST_EX + 0) * W + ps] + sb[(ST_EX + 0) * W + ps - 1]);
-          const double by = 0.25 * (sb[(ST_BY + 0) * W + ps] + sb[(ST_BY + 0) * W + ps - 1] +
-                                    sb[(ST_BYM + 0) * W + ps] + sb[(ST_BYM + 0) * W + ps - 1]);
-          acc = fl[FQ1 * W + ps] * (ex + vz * by);
-        }
+        const double n0 = fmax(fl[FN * W + sp], 0.05);
+        const double u0 = fl[FPX * W + sp] / n0;
+        ux_own = u0;
+        vz_own = fl[FPZ * W + sp] / n0;
+        if (t < TB - 1) {
+          const double n1 = fmax(fl[FN * W + sp + 1], 0.05);
+          const double u1 = fl[FPX * W + sp + 1] / n1;
+          const double e = fct_eps(u0, u1, dtdx);
+          double nu, mu;
+          fct_nu_mu(e, nu, mu);
+          wb[WB_MU * W + sp] = mu;
 #pragma unroll
-        for (int c = 1; c < 3; ++c) {
-          const double ex = 0.5 * (sb[(ST_EX + c) * W + ps] + sb[(ST_EX + c) * W + ps - 1]);
-          const double by = 0.25 * (sb[(ST_BY + c) * W + ps] + sb[(ST_BY + c) * W + ps - 1] +
-                                    sb[(ST_BYM + c) * W + ps] + sb[(ST_BYM + c) * W + ps - 1]);
-          acc = acc + fl[(FQ1 + c) * W + ps] * (ex + vz * by);
+          for (int k = 0; k < 6; ++k) {
+            const double v0 = fl[k * W + sp], v1 = fl[k * W + sp + 1];
+            wb[(WB_F + k) * W + sp] = 0.5 * e * (v0 + v1);
+            wb[(WB_D + k) * W + sp] = nu * (v1 - v0);
+          }
         }
-        sx = -acc;
-        if (warm) {
-          const double dndx = (fl[FN * W + ps + 1] - fl[FN * W + ps - 1]) / (2.0 * p.dx);
-          sx -= p.warm_T * dndx;
+        if (t >= 1 && t < TB - 1) {
+          int ps = sp;  // at a wall the clamped ghost cells carry the edge cell's source
+          if (wall) {
+            const int xg = x0 - 4 + sp;
+            ps = (xg < 0 ? 0 : (xg >= nx ? nx - 1 : xg)) - (x0 - 4);
+          }
+          const double vz = (ps == sp) ? vz_own : fl[FPZ * W + ps] / fmax(fl[FN * W + ps], 0.05);
+          double acc = 0.0;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const double ex = 0.5 * (sb[(ST_EX + c) * W + ps] + sb[(ST_EX + c) * W + ps - 1]);
+            const double by = 0.25 * (sb[(ST_BY + c) * W + ps] + sb[(ST_BY + c) * W + ps - 1] +
+                                      sb[(ST_BYM + c) * W + ps] + sb[(ST_BYM + c) * W + ps - 1]);
+            const double term = fl[(FQ1 + c) * W + ps] * (ex + vz * by);
+            acc = (c == 0) ? term : acc + term;
+          }
+          sx = -acc;
+          if (warm) {
+            const double dndx = (fl[FN * W + ps + 1] - fl[FN * W + ps - 1]) / (2.0 * p.dx);
+            sx -= p.warm_T * dndx;
+          }
         }
       }
       beam_bar(beam, TB);
 
-      // ---- B: x-sweep low-order solution at sp (FCT_Sweeps.cu:88-133).
-      {
-        const double um = wb[WB_U * W + sp - 1], u0 = wb[WB_U * W + sp], up = wb[WB_U * W + sp + 1];
-        const double eL = fct_eps(um, u0, dtdx), eR = fct_eps(u0, up, dtdx);
-        double nuL, muL, nuR, muR;
-        fct_nu_mu(eL, nuL, muL);
-        fct_nu_mu(eR, nuR, muR);
+      // ---- B: lorhot / lnrhot at sp (FCT_Sweeps.cu:102-103), t in [1, TB-1).
+      if (t >= 1 && t < TB - 1) {
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-          const double vm = fl[k * W + sp - 1], v0 = fl[k * W + sp], vp = fl[k * W + sp + 1];
-          const double fL = 0.5 * eL * (vm + v0);
-          const double fR = 0.5 * eR * (v0 + vp);
-          const double dL = nuL * (v0 - vm);
-          const double dR = nuR * (vp - v0);
-          const double lo = (k == FPX) ? v0 + dt * sx - (fR - fL) : v0 - (fR - fL);
+          const double v0 = fl[k * W + sp];
+          const double fd = wb[(WB_F + k) * W + sp] - wb[(WB_F + k) * W + sp - 1];
+          const double dd = wb[(WB_D + k) * W + sp] - wb[(WB_D + k) * W + sp - 1];
+          const double lo = (k == FPX) ? v0 + dt * sx - fd : v0 - fd;
           wb[(WB_LOR + k) * W + sp] = lo;
-          wb[(WB_LNR + k) * W + sp] = lo + (dR - dL);
+          wb[(WB_LNR + k) * W + sp] = lo + dd;
         }
       }
       beam_bar(beam, TB);
 
       // ---- C: antidiffusive flux and limiter at interface sp+1/2
-      // (FCT_Sweeps.cu:139-160), t in [1, TB-2).
-      if (t >= 1 && t < TB - 2) {
-        const double e = fct_eps(wb[WB_U * W + sp], wb[WB_U * W + sp + 1], dtdx);
-        double nu, mu;
-        fct_nu_mu(e, nu, mu);
+      // (FCT_Sweeps.cu:139-160), t in [2, TB-3).
+      if (t >= 2 && t < TB - 3) {
+        const double mu = wb[WB_MU * W + sp];
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
           const double* lor = wb + (WB_LOR + k) * W;
           const double* lnr = wb + (WB_LNR + k) * W;
           const double fad = mu * (lor[sp + 1] - lor[sp]);
           wb[(WB_FLIM + k) * W + sp] =
-              fct_limit(fad, lnr[sp] - lnr[sp - 1], lnr[sp + 1] - lnr[sp], lnr[sp + 2] - lnr[sp + 1]);
+              fct_limit_sel(fad, lnr[sp] - lnr[sp - 1], lnr[sp + 1] - lnr[sp], lnr[sp + 2] - lnr[sp + 1]);
         }
       }
       beam_bar(beam, TB);
 
       // ---- D: x-swept value of the own column, z-sources, z-pipeline.
-      if (t >= 2 && t < TB - 2) {
+      if (zthread) {
         double Vx[6];
 #pragma unroll
         for (int k = 0; k < 6; ++k)
           Vx[k] = wb[(WB_LNR + k) * W + sp] - (wb[(WB_FLIM + k) * W + sp] - wb[(WB_FLIM + k) * W + sp - 1]);
-        const double vx = wb[WB_U * W + sp];
+        const double vx = ux_own;
         const double vz = vz_own;
         const double q1 = fl[FQ1 * W + sp], q2 = fl[FQ2 * W + sp], q3 = fl[FQ3 * W + sp];
         double by[3], ezn[3], azn[3];
@@ -281,7 +336,7 @@ __global__ void __launch_bounds__(2 * TB)
           const double lo = (k >= FPZ) ? V1[k] + dt * S1[k] - (fR - f1[k]) : V1[k] - (fR - f1[k]);
           const double ln = lo + (dR - d1[k]);
           const double fad = mu1 * (lo - L2[k]);
-          const double flim = fct_limit(A2[k], N3[k] - N4[k], N2[k] - N3[k], ln - N2[k]);
+          const double flim = fct_limit_sel(A2[k], N3[k] - N4[k], N2[k] - N3[k], ln - N2[k]);
           outv[k] = N3[k] - (flim - F3[k]);
           V1[k] = Vx[k];
           S1[k] = S[k];
@@ -308,7 +363,7 @@ __global__ void __launch_bounds__(2 * TB)
         }
       }
     }
-    cp_async_wait<0>();
+    if (!bulk) cp_async_wait<0>();
   }
 }
 
@@ -324,17 +379,19 @@ static cudaError_t prepare_fct_t() {
 // (strip, segment) items round-robin.
 template <int TB, int NST>
 static cudaError_t launch_fct_t(const State& in, const State& out, const StepParams& p, int seg_len, int grid_ctas,
-                                cudaStream_t s) {
+                                bool allow_bulk, unsigned* err, cudaStream_t s) {
   FctSched sc;
-  sc.nstrips = (p.nx + (TB - 4) - 1) / (TB - 4);
+  sc.nstrips = (p.nx + (TB - 6) - 1) / (TB - 6);
   sc.seg_len = seg_len;
   sc.nitems = sc.nstrips * ((p.nz + seg_len - 1) / seg_len);
+  sc.bulk = (allow_bulk && p.periodic_x && (p.nx % 2) == 0 && p.nx >= TB + 2) ? 1 : 0;
+  sc.err = err;
   const int grid = std::min(sc.nitems, grid_ctas);
   fct_fused_kernel<TB, NST><<<grid, 2 * TB, fct_smem_bytes<TB>(NST), s>>>(in, out, p, sc);
   return cudaGetLastError();
 }
 
-constexpr int FCT_NST = 4;
+constexpr int FCT_NST = 3;
 
 cudaError_t prepare_fct(int tb) {
   switch (tb) {
@@ -357,11 +414,11 @@ int fct_ctas_per_sm(int tb) {
 }
 
 cudaError_t launch_fct(const State& in, const State& out, const StepParams& p, int tb, int seg_len, int grid_ctas,
-                       cudaStream_t s) {
+                       bool allow_bulk, unsigned* err, cudaStream_t s) {
   switch (tb) {
-    case 32: return launch_fct_t<32, FCT_NST>(in, out, p, seg_len, grid_ctas, s);
-    case 64: return launch_fct_t<64, FCT_NST>(in, out, p, seg_len, grid_ctas, s);
-    case 128: return launch_fct_t<128, FCT_NST>(in, out, p, seg_len, grid_ctas, s);
+    case 32: return launch_fct_t<32, FCT_NST>(in, out, p, seg_len, grid_ctas, allow_bulk, err, s);
+    case 64: return launch_fct_t<64, FCT_NST>(in, out, p, seg_len, grid_ctas, allow_bulk, err, s);
+    case 128: return launch_fct_t<128, FCT_NST>(in, out, p, seg_len, grid_ctas, allow_bulk, err, s);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -7,7 +7,9 @@
 //
 // Layout: work items are (x-strip of TX columns, z-segment) pairs handed to
 // persistent CTAs round-robin; a CTA streams along z with the rows it needs
-// staged in shared memory by cp.async NST-1 rows ahead.  When row q arrives
+// staged in shared memory NST-2 rows ahead (one thread issues TMA bulk row
+// copies completing on a per-stage mbarrier; wall boundaries use per-element
+// cp.async with clamped indices).  When row q arrives
 // it forms, for every column, the per-cell velocities px/n and pz/n of both
 // beams (each division done once), then Ex(q) (Jx needs row q only) and
 // Ez(q-1) (Jz needs rows q-1, q), and finally the potential and Faraday on
@@ -23,36 +25,38 @@ namespace ymkh {
 
 namespace {
 
-constexpr int MX_TX = 128;  // output columns per strip
-constexpr int MX_NT = 256;  // threads per CTA
-constexpr int MX_NST = 4;   // stage ring depth
-constexpr int MX_W = MX_TX + 2;  // stage row: position s <-> x = x0 - 1 + s
+constexpr int MX_TX = 64;        // output columns per strip
+constexpr int MX_NT = 2 * MX_TX; // threads per CTA
+constexpr int MX_NST = 4;        // stage ring depth (rows q-1, q in use)
+constexpr int MX_W = MX_TX + 4;  // stage row: position s <-> x = x0 - 2 + s
 
-// stage offsets in rows of MX_W doubles
-constexpr int MS_FL = 0;    // 12 fluid arrays, s in [1, TX+2)
-constexpr int MS_BY = 12;   // By1..3,          s in [0, TX+2)
-constexpr int MS_AZ = 15;   // Az1..3,          s in [1, TX+1)
-constexpr int MS_EX = 18;   // Ex1..3,          s in [1, TX+1)
-constexpr int MS_EZ = 21;   // Ez1..3,          s in [1, TX+2)
+// stage offsets in rows of MX_W doubles (every array staged over the full row)
+constexpr int MS_FL = 0;   // 12 fluid arrays
+constexpr int MS_BY = 12;  // By1..3
+constexpr int MS_AZ = 15;  // Az1..3
+constexpr int MS_EX = 18;  // Ex1..3
+constexpr int MS_EZ = 21;  // Ez1..3
 constexpr int MS_SIZE = 24;
 
-// work rows: per-cell velocities [2 rows][beam][vx, vz], new Ex [2 rows][3], new Ez [3]
-constexpr int MW_V = 0;     // index (row&1)*4 + beam*2 + {0: px/n, 1: pz/n}
-constexpr int MW_EX = 8;    // (row&1)*3 + c
-constexpr int MW_EZ = 14;   // c
+// work rows: per-cell velocities [2 rows][beam][px/n, pz/n], new Ex [2 rows][3], new Ez [3]
+constexpr int MW_V = 0;
+constexpr int MW_EX = 8;
+constexpr int MW_EZ = 14;
 constexpr int MW_SIZE = 17;
 
 }  // namespace
 
 constexpr size_t maxwell_smem_bytes() {
-  return (size_t)MX_W * sizeof(double) * (MX_NST * MS_SIZE + MW_SIZE) + (size_t)MX_W * sizeof(int);
+  return (size_t)MX_W * sizeof(double) * (MX_NST * MS_SIZE + MW_SIZE) + (size_t)MX_W * sizeof(int) +
+         (size_t)8 * MX_NST + 16;
 }
 
 struct MxSched {
-  int nstrips, seg_len, nitems;
+  int nstrips, seg_len, nitems, bulk;
+  unsigned* err;
 };
 
-__global__ void __launch_bounds__(MX_NT)
+__global__ void __launch_bounds__(MX_NT, 3)
     maxwell_fused_kernel(const __grid_constant__ State fluid_new, const __grid_constant__ State fields_old,
                          const __grid_constant__ State out, const __grid_constant__ StepParams p, const MxSched sc) {
   constexpr int TX = MX_TX, W = MX_W, NST = MX_NST, NT = MX_NT;
@@ -60,11 +64,21 @@ __global__ void __launch_bounds__(MX_NT)
   double* const stage = smem;
   double* const wk = smem + (size_t)NST * MS_SIZE * W;
   int* const xtab = reinterpret_cast<int*>(wk + (size_t)MW_SIZE * W);
+  uint64_t* const bars = reinterpret_cast<uint64_t*>(
+      (reinterpret_cast<uintptr_t>(xtab + W) + 15) & ~static_cast<uintptr_t>(15));
 
   const int nx = p.nx, nz = p.nz;
   const int tid = threadIdx.x;
   const bool wall = !p.periodic_x;
+  const bool bulk = sc.bulk != 0;
   const double dt = p.dt, c2 = p.c2, al = p.alpha, e0 = p.eps0;
+
+  if (bulk && tid == 0) {
+    for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  unsigned issued = 0, consumed = 0;
 
   for (int item = blockIdx.x; item < sc.nitems; item += gridDim.x) {
     const int x0 = (item % sc.nstrips) * TX;
@@ -72,56 +86,71 @@ __global__ void __launch_bounds__(MX_NT)
     const int ze = min(nz, zs + sc.seg_len);
 
     __syncthreads();
-    for (int i = tid; i < W; i += NT) xtab[i] = xmap(x0 - 1 + i, nx, p.periodic_x);
+    for (int i = tid; i < W; i += NT) xtab[i] = xmap(x0 - 2 + i, nx, p.periodic_x);
     __syncthreads();
 
-    auto issue_row = [&](int q, int s) {
+    auto issue_row = [&](int q) {
+      const int s = (int)(issued % NST);
       double* sb = stage + (size_t)s * MS_SIZE * W;
       const size_t ro = (size_t)zwrap(q, nz) * nx;
-      for (int i = tid; i < 12 * (TX + 1); i += NT) {
-        const int a = i / (TX + 1), k = i - a * (TX + 1);
-        const double* src = (a < 6 ? fluid_new.a[a] : fluid_new.b[a - 6]) + ro + xtab[1 + k];
-        cp_async8(sb + (MS_FL + a) * W + 1 + k, src);
+      if (bulk) {
+        if (tid == 0) {
+          mbar_expect_tx(&bars[s], (unsigned)(MS_SIZE * W * 8));
+          for (int a = 0; a < 12; ++a)
+            bulk_row_periodic(sb + (MS_FL + a) * W, (a < 6 ? fluid_new.a[a] : fluid_new.b[a - 6]) + ro, x0 - 2, W,
+                              nx, &bars[s]);
+          for (int c = 0; c < 3; ++c) {
+            bulk_row_periodic(sb + (MS_BY + c) * W, fields_old.f[BY1 + c] + ro, x0 - 2, W, nx, &bars[s]);
+            bulk_row_periodic(sb + (MS_AZ + c) * W, fields_old.f[AZ1 + c] + ro, x0 - 2, W, nx, &bars[s]);
+            bulk_row_periodic(sb + (MS_EX + c) * W, fields_old.f[EX1 + c] + ro, x0 - 2, W, nx, &bars[s]);
+            bulk_row_periodic(sb + (MS_EZ + c) * W, fields_old.f[EZ1 + c] + ro, x0 - 2, W, nx, &bars[s]);
+          }
+        }
+      } else {
+        for (int i = tid; i < MS_SIZE * W; i += NT) {
+          const int a = i / W, k = i - a * W;
+          const double* base;
+          if (a < 12)
+            base = (a < 6) ? fluid_new.a[a] : fluid_new.b[a - 6];
+          else {
+            const int kind = (a - 12) / 3, c = (a - 12) % 3;
+            base = (kind == 0) ? fields_old.f[BY1 + c]
+                   : (kind == 1) ? fields_old.f[AZ1 + c]
+                   : (kind == 2) ? fields_old.f[EX1 + c]
+                                 : fields_old.f[EZ1 + c];
+          }
+          cp_async8(sb + a * W + k, base + ro + xtab[k]);
+        }
+        cp_async_commit();
       }
-      for (int i = tid; i < 3 * W; i += NT) {
-        const int c = i / W, k = i - c * W;
-        cp_async8(sb + (MS_BY + c) * W + k, fields_old.f[BY1 + c] + ro + xtab[k]);
-      }
-      for (int i = tid; i < 6 * TX; i += NT) {
-        const int a = i / TX, k = i - a * TX;
-        const double* base = (a < 3) ? fields_old.f[AZ1 + a] : fields_old.f[EX1 + a - 3];
-        cp_async8(sb + (MS_AZ + a) * W + 1 + k, base + ro + xtab[1 + k]);
-      }
-      for (int i = tid; i < 3 * (TX + 1); i += NT) {
-        const int c = i / (TX + 1), k = i - c * (TX + 1);
-        cp_async8(sb + (MS_EZ + c) * W + 1 + k, fields_old.f[EZ1 + c] + ro + xtab[1 + k]);
-      }
+      ++issued;
     };
 
     // Rows q-1 and q are read in the same iteration, so NST-2 rows are in
     // flight and the refill goes to the stage of row q-2.
     const int q_first = zs - 1, q_last = ze;
-#pragma unroll
-    for (int k = 0; k < NST - 2; ++k) {
-      if (q_first + k <= q_last) issue_row(q_first + k, k);
-      cp_async_commit();
-    }
+    for (int k = 0; k < NST - 2; ++k)
+      if (q_first + k <= q_last) issue_row(q_first + k);
+      else if (!bulk) cp_async_commit();
 
-    for (int q = q_first, it = 0; q <= q_last; ++q, ++it) {
-      cp_async_wait<NST - 3>();
+    for (int q = q_first; q <= q_last; ++q) {
+      const int s = (int)(consumed % NST);
+      const int sprev = (int)((consumed + NST - 1) % NST);
+      if (bulk)
+        mbar_wait(&bars[s], (consumed / NST) & 1u, sc.err);
+      else
+        cp_async_wait<NST - 3>();
       __syncthreads();  // row q staged by every thread; row q-2's stage is free
-      {
-        const int qn = q + NST - 2;
-        if (qn <= q_last) issue_row(qn, (it + NST - 2) % NST);
-        cp_async_commit();
-      }
-      const double* sb = stage + (size_t)(it % NST) * MS_SIZE * W;                 // row q
-      const double* sp = stage + (size_t)((it + NST - 1) % NST) * MS_SIZE * W;     // row q-1
+      ++consumed;
+      if (q + NST - 2 <= q_last) issue_row(q + NST - 2);
+      else if (!bulk) cp_async_commit();
+      const double* sb = stage + (size_t)s * MS_SIZE * W;      // row q
+      const double* sp = stage + (size_t)sprev * MS_SIZE * W;  // row q-1
       const int rq = q & 1, rp = (q - 1) & 1;
 
-      // ---- 1: per-cell velocities of row q (YM_Physics.cu:22-25, 38-41)
+      // ---- 1: per-cell velocities of row q at x in [x0, x0+TX] (YM_Physics.cu:22-25, 38-41)
       for (int i = tid; i < 2 * (TX + 1); i += NT) {
-        const int b = i / (TX + 1), k = 1 + (i - b * (TX + 1));
+        const int b = i / (TX + 1), k = 2 + (i - b * (TX + 1));
         const double* fl = sb + (size_t)(MS_FL + 6 * b) * W;
         const double n = fmax(fl[FN * W + k], 1e-10);
         wk[(MW_V + rq * 4 + b * 2 + 0) * W + k] = fl[FPX * W + k] / n;
@@ -129,9 +158,9 @@ __global__ void __launch_bounds__(MX_NT)
       }
       __syncthreads();
 
-      // ---- 2a: Ampère for Ex on row q, columns [x0, x0+TX) (threads [0, TX))
       if (tid < TX) {
-        const int k = 1 + tid;
+        // ---- 2a: Ampère for Ex on row q, column x0+tid
+        const int k = 2 + tid;
         double nq[2][3], vxr[2];
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
@@ -142,21 +171,19 @@ __global__ void __launch_bounds__(MX_NT)
           for (int a = 0; a < 3; ++a) nq[b][a] = 0.5 * (n0 * fl[(FQ1 + a) * W + k] + n1 * fl[(FQ1 + a) * W + k + 1]);
         }
         const double by1 = sb[(MS_BY + 0) * W + k], by2 = sb[(MS_BY + 1) * W + k], by3 = sb[(MS_BY + 2) * W + k];
-        const double d1 = (by1 - sp[(MS_BY + 0) * W + k]) / p.dz;
-        const double d2 = (by2 - sp[(MS_BY + 1) * W + k]) / p.dz;
-        const double d3 = (by3 - sp[(MS_BY + 2) * W + k]) / p.dz;
+        const double dz3[3] = {(by1 - sp[(MS_BY + 0) * W + k]) / p.dz, (by2 - sp[(MS_BY + 1) * W + k]) / p.dz,
+                               (by3 - sp[(MS_BY + 2) * W + k]) / p.dz};
         const double a1 = sb[(MS_AZ + 0) * W + k], a2 = sb[(MS_AZ + 1) * W + k], a3 = sb[(MS_AZ + 2) * W + k];
         const double kx[3] = {a2 * by3 - a3 * by2, a3 * by1 - a1 * by3, a1 * by2 - a2 * by1};
-        const double dz3[3] = {d1, d2, d3};
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
           const double jx = -(nq[0][a] * vxr[0] + nq[1][a] * vxr[1]);
           wk[(MW_EX + rq * 3 + a) * W + k] = sb[(MS_EX + a) * W + k] + dt * (c2 * (-dz3[a] - al * kx[a]) - jx / e0);
         }
       } else {
-        // ---- 2b: Ampère for Ez on row q-1, columns [x0, x0+TX] (threads [TX, 2TX) + one extra)
+        // ---- 2b: Ampère for Ez on row q-1, columns [x0, x0+TX]
         for (int i = tid - TX; i < TX + 1; i += NT - TX) {
-          const int k = 1 + i;
+          const int k = 2 + i;
           double nqz[2][3], vzt[2];
 #pragma unroll
           for (int b = 0; b < 2; ++b) {
@@ -184,16 +211,16 @@ __global__ void __launch_bounds__(MX_NT)
       // (YM_Physics.cu:127): its Ez is that column's new Ez.
       if (wall && x0 + TX >= nx) {
         if (tid < 3) {
-          const int kl = 1 + (nx - 1 - x0);
+          const int kl = 2 + (nx - 1 - x0);
           wk[(MW_EZ + tid) * W + kl + 1] = wk[(MW_EZ + tid) * W + kl];
         }
         __syncthreads();
       }
 
-      // ---- 3: potential and Faraday on row q-1 (threads [0, TX))
+      // ---- 3: potential and Faraday on row q-1
       const int o = q - 1;
       if (tid < TX && o >= zs && o < ze && x0 + tid < nx) {
-        const int k = 1 + tid;
+        const int k = 2 + tid;
         const size_t gi = idx2(x0 + tid, o, nx);
         double az[3], ex[3], ez[3];
 #pragma unroll
@@ -218,7 +245,7 @@ __global__ void __launch_bounds__(MX_NT)
         }
       }
     }
-    cp_async_wait<0>();
+    if (!bulk) cp_async_wait<0>();
   }
 }
 
@@ -233,12 +260,16 @@ int maxwell_ctas_per_sm() {
   return n;
 }
 
+int maxwell_strip_width() { return MX_TX; }
+
 cudaError_t launch_maxwell(const State& fluid_new, const State& fields_old, const State& out, const StepParams& p,
-                           int seg_len, int grid_ctas, cudaStream_t s) {
+                           int seg_len, int grid_ctas, bool allow_bulk, unsigned* err, cudaStream_t s) {
   MxSched sc;
   sc.nstrips = (p.nx + MX_TX - 1) / MX_TX;
   sc.seg_len = seg_len;
   sc.nitems = sc.nstrips * ((p.nz + seg_len - 1) / seg_len);
+  sc.bulk = (allow_bulk && p.periodic_x && (p.nx % 2) == 0 && p.nx >= MX_W) ? 1 : 0;
+  sc.err = err;
   const int grid = std::min(sc.nitems, grid_ctas);
   maxwell_fused_kernel<<<grid, MX_NT, maxwell_smem_bytes(), s>>>(fluid_new, fields_old, out, p, sc);
   return cudaGetLastError();

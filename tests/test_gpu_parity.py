@@ -138,9 +138,11 @@ def test_energy_and_mode_amp(cuda, ref, orc, name):
     assert abs(e_gpu - e_ref) <= 1e-13 * abs(e_ref)
     a_gpu = np.array(run.mode_amp(1))
     a_orc = np.array(orc.mode_amp(g, s, 1))
-    # the conjugate amplitude of a circularly polarised seed is a
-    # cancellation residue: compare both against the main amplitude's scale
-    assert np.all(np.abs(a_gpu - a_orc) <= 1e-12 * np.abs(a_orc).max()), (a_gpu, a_orc)
+    # amplitudes can be cancellation residues (the conjugate of a circular
+    # seed; a mode the band filter removes): compare on the scale of the
+    # column DFT's input, the Az2/Az3 rms
+    scale = np.sqrt(np.mean(s[10] ** 2 + s[11] ** 2))
+    assert np.all(np.abs(a_gpu - a_orc) <= 1e-12 * max(np.abs(a_orc).max(), scale)), (a_gpu, a_orc)
     run.close()
 
 
