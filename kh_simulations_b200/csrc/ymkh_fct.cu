@@ -141,26 +141,31 @@ __global__ void __launch_bounds__(2 * TB)
       const int zp = (zr == nz - 1) ? 0 : zr + 1;
       const size_t ro = (size_t)zr * nx, rom = (size_t)zm * nx, rop = (size_t)zp * nx;
       if (bulk) {
-        if (tid == 0) {
+        if (tid < 32) {  // warp 0: lane 0 arms the stage, then each lane copies whole rows
           const int narr = 33 + (warm ? 4 : 0);
-          mbar_expect_tx(&bars[s], (unsigned)(narr * W * 8));
+          if (tid == 0) mbar_expect_tx(&bars[s], (unsigned)(narr * W * 8));
+          __syncwarp();
           const int xs = x0 - 4;
-          for (int a = 0; a < 12; ++a)
-            bulk_row_periodic(sb + (ST_FL + a) * W, (a < 6 ? st.a[a] : st.b[a - 6]) + ro, xs, W, nx, &bars[s]);
-          for (int c = 0; c < 3; ++c) {
-            bulk_row_periodic(sb + (ST_EX + c) * W, st.f[EX1 + c] + ro, xs, W, nx, &bars[s]);
-            bulk_row_periodic(sb + (ST_BY + c) * W, st.f[BY1 + c] + ro, xs, W, nx, &bars[s]);
-            bulk_row_periodic(sb + (ST_BYM + c) * W, st.f[BY1 + c] + rom, xs, W, nx, &bars[s]);
-            bulk_row_periodic(sb + (ST_EZ + c) * W, st.f[EZ1 + c] + ro, xs, W, nx, &bars[s]);
-            bulk_row_periodic(sb + (ST_EZM + c) * W, st.f[EZ1 + c] + rom, xs, W, nx, &bars[s]);
-            bulk_row_periodic(sb + (ST_AZ + c) * W, st.f[AZ1 + c] + ro, xs, W, nx, &bars[s]);
-            bulk_row_periodic(sb + (ST_AZM + c) * W, st.f[AZ1 + c] + rom, xs, W, nx, &bars[s]);
-          }
-          if (warm) {
-            bulk_row_periodic(sb + (ST_NZP + 0) * W, st.a[FN] + rop, xs, W, nx, &bars[s]);
-            bulk_row_periodic(sb + (ST_NZP + 1) * W, st.b[FN] + rop, xs, W, nx, &bars[s]);
-            bulk_row_periodic(sb + (ST_NZM + 0) * W, st.a[FN] + rom, xs, W, nx, &bars[s]);
-            bulk_row_periodic(sb + (ST_NZM + 1) * W, st.b[FN] + rom, xs, W, nx, &bars[s]);
+          for (int a = tid; a < narr; a += 32) {
+            const double* row;
+            int dsto;
+            if (a < 12) {
+              row = (a < 6 ? st.a[a] : st.b[a - 6]) + ro;
+              dsto = ST_FL + a;
+            } else if (a < 33) {
+              const int kind = (a - 12) / 3, c = (a - 12) - kind * 3;  // EX, BY, BYM, EZ, EZM, AZ, AZM
+              const double* base = (kind == 0) ? st.f[EX1 + c]
+                                   : (kind <= 2) ? st.f[BY1 + c]
+                                   : (kind <= 4) ? st.f[EZ1 + c]
+                                                 : st.f[AZ1 + c];
+              row = base + ((kind == 2 || kind == 4 || kind == 6) ? rom : ro);
+              dsto = ST_EX + (a - 12);
+            } else {
+              const int w = a - 33;  // NZP A, NZP B, NZM A, NZM B
+              row = ((w & 1) ? st.b[FN] : st.a[FN]) + ((w >> 1) ? rom : rop);
+              dsto = ST_NZP + w;
+            }
+            bulk_row_periodic(sb + dsto * W, row, xs, W, nx, &bars[s]);
           }
         }
       } else {

@@ -72,6 +72,9 @@ __global__ void __launch_bounds__(MX_NT, 3)
   const bool wall = !p.periodic_x;
   const bool bulk = sc.bulk != 0;
   const double dt = p.dt, c2 = p.c2, al = p.alpha, e0 = p.eps0;
+  // c = eps_0 = 1 (ymgpu2d/main_ym.cu:69): 1*x and x/1 are exact, so the
+  // products and quotients by them can be skipped without changing a bit
+  const bool unit = (c2 == 1.0 && e0 == 1.0);
 
   if (bulk && tid == 0) {
     for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
@@ -94,16 +97,21 @@ __global__ void __launch_bounds__(MX_NT, 3)
       double* sb = stage + (size_t)s * MS_SIZE * W;
       const size_t ro = (size_t)zwrap(q, nz) * nx;
       if (bulk) {
-        if (tid == 0) {
-          mbar_expect_tx(&bars[s], (unsigned)(MS_SIZE * W * 8));
-          for (int a = 0; a < 12; ++a)
-            bulk_row_periodic(sb + (MS_FL + a) * W, (a < 6 ? fluid_new.a[a] : fluid_new.b[a - 6]) + ro, x0 - 2, W,
-                              nx, &bars[s]);
-          for (int c = 0; c < 3; ++c) {
-            bulk_row_periodic(sb + (MS_BY + c) * W, fields_old.f[BY1 + c] + ro, x0 - 2, W, nx, &bars[s]);
-            bulk_row_periodic(sb + (MS_AZ + c) * W, fields_old.f[AZ1 + c] + ro, x0 - 2, W, nx, &bars[s]);
-            bulk_row_periodic(sb + (MS_EX + c) * W, fields_old.f[EX1 + c] + ro, x0 - 2, W, nx, &bars[s]);
-            bulk_row_periodic(sb + (MS_EZ + c) * W, fields_old.f[EZ1 + c] + ro, x0 - 2, W, nx, &bars[s]);
+        if (tid < 32) {  // warp 0: lane 0 arms the stage, then each lane copies whole rows
+          if (tid == 0) mbar_expect_tx(&bars[s], (unsigned)(MS_SIZE * W * 8));
+          __syncwarp();
+          for (int a = tid; a < MS_SIZE; a += 32) {
+            const double* base;
+            if (a < 12)
+              base = (a < 6) ? fluid_new.a[a] : fluid_new.b[a - 6];
+            else {
+              const int kind = (a - 12) / 3, c = (a - 12) % 3;
+              base = (kind == 0) ? fields_old.f[BY1 + c]
+                     : (kind == 1) ? fields_old.f[AZ1 + c]
+                     : (kind == 2) ? fields_old.f[EX1 + c]
+                                   : fields_old.f[EZ1 + c];
+            }
+            bulk_row_periodic(sb + a * W, base + ro, x0 - 2, W, nx, &bars[s]);
           }
         }
       } else {
@@ -178,7 +186,8 @@ __global__ void __launch_bounds__(MX_NT, 3)
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
           const double jx = -(nq[0][a] * vxr[0] + nq[1][a] * vxr[1]);
-          wk[(MW_EX + rq * 3 + a) * W + k] = sb[(MS_EX + a) * W + k] + dt * (c2 * (-dz3[a] - al * kx[a]) - jx / e0);
+          const double rhs = unit ? (-dz3[a] - al * kx[a]) - jx : c2 * (-dz3[a] - al * kx[a]) - jx / e0;
+          wk[(MW_EX + rq * 3 + a) * W + k] = sb[(MS_EX + a) * W + k] + dt * rhs;
         }
       } else {
         // ---- 2b: Ampère for Ez on row q-1, columns [x0, x0+TX]
@@ -202,7 +211,7 @@ __global__ void __launch_bounds__(MX_NT, 3)
             const double by = sp[(MS_BY + a) * W + k];
             const double dbx = (by - sp[(MS_BY + a) * W + k - 1]) / p.dx;
             const double ez0 = wz ? 0.0 : sp[(MS_EZ + a) * W + k];
-            wk[(MW_EZ + a) * W + k] = ez0 + dt * (c2 * dbx - jz / e0);
+            wk[(MW_EZ + a) * W + k] = ez0 + dt * (unit ? dbx - jz : c2 * dbx - jz / e0);
           }
         }
       }

@@ -181,8 +181,10 @@ def test_long_history_vs_oracle(cuda, orc):
 
 def test_10k_step_history_vs_reference(cuda, ref):
     """The headline single-run configuration (NZ = 256, NX = 512, keep
-    |k| <= 85): energy history every 10 steps over 10^4 steps agrees with the
-    reference's own kernels to 1e-9, mode-1 amplitude too."""
+    |k| <= 85): the energy history every 10 steps agrees with the
+    reference's own kernels to 1e-9 over 10^4 steps or until the reference's
+    halt rule (NaN/Inf or E/E0 > 100, ymgpu2d/main_ym.cu:249, 467-474) stops
+    the run; both must halt at the same check.  Mode-1 amplitude likewise."""
     from kh_simulations_b200._lib import Grid
     from kh_simulations_b200.config import derive, loads, step_params
     from kh_simulations_b200.run import KHRun, init_params
@@ -197,20 +199,28 @@ def test_10k_step_history_vs_reference(cuda, ref):
     ref.init(ip)
     run = KHRun(cfg)
     run.init()
-    er, eg = [], []
+    e0r, e0g = ref.energy(), run.energy()
+    er, eg, ar, ag = [], [], [], []
+    halted_r = halted_g = False
     for _ in range(1000):
         ref.step(10)
         run.step(10)
-        er.append(ref.energy())
-        eg.append(run.energy())
+        a, b = ref.energy(), run.energy()
+        halted_r = not np.isfinite(a) or a / e0r > d.energy_thresh
+        halted_g = not np.isfinite(b) or b / e0g > d.energy_thresh
+        if halted_r or halted_g:
+            break
+        er.append(a)
+        eg.append(b)
+        sr = ref.get_state() if len(er) % 100 == 0 else None
+        if sr is not None:
+            ar.append(np.abs(np.fft.fft(sr[10] + 1j * sr[11], axis=0)[1]).mean() / d.nz)
+            ag.append(run.mode_amp(1)[0])
+    assert halted_r == halted_g, (halted_r, halted_g, len(er))
     er, eg = np.array(er), np.array(eg)
-    assert np.isfinite(er).all()
+    assert len(er) >= 100
     dev = np.abs(eg - er) / np.abs(er)
-    assert dev.max() < 1e-9, (dev.max(), int(dev.argmax()))
-    sr = ref.get_state()
-    sg = run.state_numpy()
-    from kh_simulations_b200.run import KHRun as _K  # noqa: F401
-    a_ref = np.abs(np.fft.fft(sr[10] + 1j * sr[11], axis=0)[1]).mean() / d.nz
-    a_gpu = run.mode_amp(1)[0]
-    assert abs(a_gpu - a_ref) < 1e-9 * a_ref
+    assert dev.max() < 1e-9, (dev.max(), int(dev.argmax()), len(er))
+    ar, ag = np.array(ar), np.array(ag)
+    assert np.all(np.abs(ag - ar) <= 1e-9 * np.abs(ar)), (ar, ag)
     run.close()
