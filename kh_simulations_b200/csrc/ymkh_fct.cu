@@ -53,10 +53,11 @@ constexpr int ST_SIZE = 37;
 // Per-beam work arrays (units of W), by stage position / interface index
 // (interface j+1/2 stored at j).  Fluxes F, D are dead after phase B, so the
 // limited fluxes reuse their space.
-constexpr int WB_MU = 0, WB_F = 1, WB_D = 7, WB_FLIM = 1, WB_LOR = 13, WB_LNR = 19, WB_SIZE = 25;
+constexpr int WB_F = 1, WB_D = 7, WB_FLIM = 1, WB_LOR = 13, WB_LNR = 19, WB_SIZE = 25;
 
-__device__ __forceinline__ void beam_bar(int beam, int nthreads) {
-  asm volatile("bar.sync %0, %1;" ::"r"(beam + 1), "r"(nthreads) : "memory");
+// Named barrier of one (beam, half) thread group (ids 1..4; 0 is __syncthreads).
+__device__ __forceinline__ void beam_bar(int group, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(group + 1), "r"(nthreads) : "memory");
 }
 
 // apply_fct_limiter (FCT_DeviceMath.cuh:108-125) with the products by
@@ -85,12 +86,19 @@ struct FctSched {
   unsigned* err; // device error word (bounded waits that ran out)
 };
 
+// Per-thread z-pipeline state for the three swept variables of one half
+// (H = 0: n, px, pz; H = 1: Q1, Q2, Q3) of one beam.
+struct ZPipe {
+  double V1[3], f1[3], d1[3], L2[3], N4[3], N3[3], N2[3], A2[3], F3[3], S1[3];
+  double U1, mu1;
+};
+
 template <int TB, int NST>
-__global__ void __launch_bounds__(2 * TB)
+__global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
     fct_fused_kernel(const __grid_constant__ State st, const __grid_constant__ State out,
                      const __grid_constant__ StepParams p, const FctSched sc) {
   constexpr int W = TB + 2;
-  constexpr int NT = 2 * TB;
+  constexpr int NT = 4 * TB;
   constexpr int TO = TB - 6;  // output columns per strip
   extern __shared__ __align__(16) double smem[];
   double* const stage = smem;
@@ -101,9 +109,11 @@ __global__ void __launch_bounds__(2 * TB)
 
   const int nx = p.nx, nz = p.nz;
   const int tid = threadIdx.x;
-  const int beam = tid / TB;
-  const int t = tid - beam * TB;
-  const int sp = t + 1;  // this thread's stage position
+  const int grp = tid / TB;     // (beam, half) group, 0..3
+  const int beam = grp >> 1;
+  const int half = grp & 1;     // 0: n, px, pz   1: Q1, Q2, Q3
+  const int t = tid - grp * TB;
+  const int sp = t + 1;         // this thread's stage position
   const bool warm = p.warm_T > 0.0;
   const bool wall = !p.periodic_x;
   const bool bulk = sc.bulk != 0;
@@ -111,6 +121,7 @@ __global__ void __launch_bounds__(2 * TB)
   const double dtdx = p.dt / p.dx;
   const double dtdz = p.dt / p.dz;
   double* const wb = wk + (size_t)beam * WB_SIZE * W;
+  const int k0 = 3 * half;      // first swept variable of this half
 
   if (bulk && tid == 0) {
     for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
@@ -130,9 +141,6 @@ __global__ void __launch_bounds__(2 * TB)
       for (int i = tid; i < W; i += NT) xtab[i] = xmap(x0 - 4 + i, nx, p.periodic_x);
     __syncthreads();
 
-    // Stage one row (clamped z index).  Bulk path: thread 0 arms the stage's
-    // mbarrier and issues whole-row copies; element path: every thread
-    // issues 8-byte cp.async with clamped shear indices.
     auto issue_row = [&](int r) {
       const int s = (int)(issued % NST);
       double* sb = stage + (size_t)s * ST_SIZE * W;
@@ -200,20 +208,23 @@ __global__ void __launch_bounds__(2 * TB)
       if (r_first + k <= r_last) issue_row(r_first + k);
       else if (!bulk) cp_async_commit();
 
-    double V1[6], f1[6], d1[6], L2[6], N4[6], N3[6], N2[6], A2[6], F3[6], S1[6];
+    ZPipe zp;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) V1[k] = f1[k] = d1[k] = L2[k] = N4[k] = N3[k] = N2[k] = A2[k] = F3[k] = S1[k] = 0.0;
-    double U1 = 0.0, mu1 = 0.0;
+    for (int j = 0; j < 3; ++j)
+      zp.V1[j] = zp.f1[j] = zp.d1[j] = zp.L2[j] = zp.N4[j] = zp.N3[j] = zp.N2[j] = zp.A2[j] = zp.F3[j] = zp.S1[j] = 0.0;
+    zp.U1 = zp.mu1 = 0.0;
     const int x_own = x0 - 4 + sp;
-    const bool zthread = (t >= 3) && (t < TB - 3);          // owns an output column
+    const bool zthread = (t >= 3) && (t < TB - 3);  // owns an output column
     const bool owner = zthread && (x_own < nx);
 
     for (int r = r_first; r <= r_last; ++r) {
       const int s = (int)(consumed % NST);
-      if (bulk)
-        mbar_wait(&bars[s], (consumed / NST) & 1u, sc.err);
-      else
+      if (bulk) {  // one thread polls the stage's mbarrier; the CTA barrier below
+        // releases the others after it (no spinning by every thread)
+        if (tid == 0) mbar_wait(&bars[s], (consumed / NST) & 1u, sc.err);
+      } else {
         cp_async_wait<NST - 2>();
+      }
       __syncthreads();  // row r staged for everyone; the previous row's stage is free
       ++consumed;
       if (r + NST - 1 <= r_last) issue_row(r + NST - 1);
@@ -222,29 +233,29 @@ __global__ void __launch_bounds__(2 * TB)
       const double* fl = sb + (size_t)(ST_FL + beam * 6) * W;
 
       // ---- A: velocities at sp, sp+1 (YM_Fluid.cu:3-11); interface sp+1/2:
-      // eps, nu, mu and the low-order fluxes (FCT_Sweeps.cu:88-98); px
-      // source at sp (YM_Fluid.cu:43-66, 71-80).
-      double vz_own = 0.0, ux_own = 0.0, sx = 0.0;
+      // eps, nu, mu and the low-order fluxes of this half's variables
+      // (FCT_Sweeps.cu:88-98); half 0 also forms the px source at sp
+      // (YM_Fluid.cu:43-66, 71-80).
+      double vz_own, ux_own, mu_if = 0.0, sx = 0.0;
       {
         const double n0 = fmax(fl[FN * W + sp], 0.05);
-        const double u0 = fl[FPX * W + sp] / n0;
-        ux_own = u0;
+        ux_own = fl[FPX * W + sp] / n0;
         vz_own = fl[FPZ * W + sp] / n0;
         if (t < TB - 1) {
           const double n1 = fmax(fl[FN * W + sp + 1], 0.05);
           const double u1 = fl[FPX * W + sp + 1] / n1;
-          const double e = fct_eps(u0, u1, dtdx);
-          double nu, mu;
-          fct_nu_mu(e, nu, mu);
-          wb[WB_MU * W + sp] = mu;
+          const double e = fct_eps(ux_own, u1, dtdx);
+          double nu;
+          fct_nu_mu(e, nu, mu_if);
 #pragma unroll
-          for (int k = 0; k < 6; ++k) {
+          for (int j = 0; j < 3; ++j) {
+            const int k = k0 + j;
             const double v0 = fl[k * W + sp], v1 = fl[k * W + sp + 1];
             wb[(WB_F + k) * W + sp] = 0.5 * e * (v0 + v1);
             wb[(WB_D + k) * W + sp] = nu * (v1 - v0);
           }
         }
-        if (t >= 1 && t < TB - 1) {
+        if (half == 0 && t >= 1 && t < TB - 1) {
           int ps = sp;  // at a wall the clamped ghost cells carry the edge cell's source
           if (wall) {
             const int xg = x0 - 4 + sp;
@@ -267,12 +278,13 @@ __global__ void __launch_bounds__(2 * TB)
           }
         }
       }
-      beam_bar(beam, TB);
+      beam_bar(grp, TB);
 
       // ---- B: lorhot / lnrhot at sp (FCT_Sweeps.cu:102-103), t in [1, TB-1).
       if (t >= 1 && t < TB - 1) {
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
+        for (int j = 0; j < 3; ++j) {
+          const int k = k0 + j;
           const double v0 = fl[k * W + sp];
           const double fd = wb[(WB_F + k) * W + sp] - wb[(WB_F + k) * W + sp - 1];
           const double dd = wb[(WB_D + k) * W + sp] - wb[(WB_D + k) * W + sp - 1];
@@ -281,90 +293,99 @@ __global__ void __launch_bounds__(2 * TB)
           wb[(WB_LNR + k) * W + sp] = lo + dd;
         }
       }
-      beam_bar(beam, TB);
+      beam_bar(grp, TB);
 
       // ---- C: antidiffusive flux and limiter at interface sp+1/2
       // (FCT_Sweeps.cu:139-160), t in [2, TB-3).
       if (t >= 2 && t < TB - 3) {
-        const double mu = wb[WB_MU * W + sp];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
+        for (int j = 0; j < 3; ++j) {
+          const int k = k0 + j;
           const double* lor = wb + (WB_LOR + k) * W;
           const double* lnr = wb + (WB_LNR + k) * W;
-          const double fad = mu * (lor[sp + 1] - lor[sp]);
+          const double fad = mu_if * (lor[sp + 1] - lor[sp]);
           wb[(WB_FLIM + k) * W + sp] =
               fct_limit_sel(fad, lnr[sp] - lnr[sp - 1], lnr[sp + 1] - lnr[sp], lnr[sp + 2] - lnr[sp + 1]);
         }
       }
-      beam_bar(beam, TB);
+      beam_bar(grp, TB);
 
-      // ---- D: x-swept value of the own column, z-sources, z-pipeline.
+      // ---- D: x-swept values of the own column, z-sources, z-pipeline.
       if (zthread) {
-        double Vx[6];
+        double Vx[3], S[3];
 #pragma unroll
-        for (int k = 0; k < 6; ++k)
-          Vx[k] = wb[(WB_LNR + k) * W + sp] - (wb[(WB_FLIM + k) * W + sp] - wb[(WB_FLIM + k) * W + sp - 1]);
-        const double vx = ux_own;
+        for (int j = 0; j < 3; ++j) {
+          const int k = k0 + j;
+          Vx[j] = wb[(WB_LNR + k) * W + sp] - (wb[(WB_FLIM + k) * W + sp] - wb[(WB_FLIM + k) * W + sp - 1]);
+        }
         const double vz = vz_own;
         const double q1 = fl[FQ1 * W + sp], q2 = fl[FQ2 * W + sp], q3 = fl[FQ3 * W + sp];
-        double by[3], ezn[3], azn[3];
+        if (half == 0) {
+          // YM_Fluid.cu:67 (src.pz) and :76-79 (warm closure)
+          const double vx = ux_own;
+          double by[3], ezn[3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          by[c] = 0.25 * (sb[(ST_BY + c) * W + sp] + sb[(ST_BY + c) * W + sp - 1] + sb[(ST_BYM + c) * W + sp] +
-                          sb[(ST_BYM + c) * W + sp - 1]);
-          ezn[c] = 0.5 * (sb[(ST_EZ + c) * W + sp] + sb[(ST_EZM + c) * W + sp]);
-          azn[c] = 0.5 * (sb[(ST_AZ + c) * W + sp] + sb[(ST_AZM + c) * W + sp]);
+          for (int c = 0; c < 3; ++c) {
+            by[c] = 0.25 * (sb[(ST_BY + c) * W + sp] + sb[(ST_BY + c) * W + sp - 1] + sb[(ST_BYM + c) * W + sp] +
+                            sb[(ST_BYM + c) * W + sp - 1]);
+            ezn[c] = 0.5 * (sb[(ST_EZ + c) * W + sp] + sb[(ST_EZM + c) * W + sp]);
+          }
+          double sz = -(q1 * (ezn[0] - vx * by[0]) + q2 * (ezn[1] - vx * by[1]) + q3 * (ezn[2] - vx * by[2]));
+          if (warm) {
+            const double dndz = (sb[(ST_NZP + beam) * W + sp] - sb[(ST_NZM + beam) * W + sp]) / (2.0 * p.dz);
+            sz -= p.warm_T * dndz;
+          }
+          S[0] = 0.0;
+          S[1] = 0.0;
+          S[2] = sz;
+        } else {
+          // YM_Fluid.cu:99-107 (colour precession)
+          double azn[3];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) azn[c] = 0.5 * (sb[(ST_AZ + c) * W + sp] + sb[(ST_AZM + c) * W + sp]);
+          S[0] = p.alpha * vz * (q2 * azn[2] - q3 * azn[1]);
+          S[1] = p.alpha * vz * (q3 * azn[0] - q1 * azn[2]);
+          S[2] = p.alpha * vz * (q1 * azn[1] - q2 * azn[0]);
         }
-        // YM_Fluid.cu:67 (src.pz) and :76-79 (warm closure)
-        double sz = -(q1 * (ezn[0] - vx * by[0]) + q2 * (ezn[1] - vx * by[1]) + q3 * (ezn[2] - vx * by[2]));
-        if (warm) {
-          const double dndz = (sb[(ST_NZP + beam) * W + sp] - sb[(ST_NZM + beam) * W + sp]) / (2.0 * p.dz);
-          sz -= p.warm_T * dndz;
-        }
-        // YM_Fluid.cu:99-107 (colour precession)
-        double S[6];
-        S[FN] = 0.0;
-        S[FPX] = 0.0;
-        S[FPZ] = sz;
-        S[FQ1] = p.alpha * vz * (q2 * azn[2] - q3 * azn[1]);
-        S[FQ2] = p.alpha * vz * (q3 * azn[0] - q1 * azn[2]);
-        S[FQ3] = p.alpha * vz * (q1 * azn[1] - q2 * azn[0]);
 
-        const double e = fct_eps(U1, vz, dtdz);
+        const double e = fct_eps(zp.U1, vz, dtdz);
         double nu, mu;
         fct_nu_mu(e, nu, mu);
-        double outv[6];
+        double outv[3];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-          const double fR = 0.5 * e * (V1[k] + Vx[k]);
-          const double dR = nu * (Vx[k] - V1[k]);
-          const double lo = (k >= FPZ) ? V1[k] + dt * S1[k] - (fR - f1[k]) : V1[k] - (fR - f1[k]);
-          const double ln = lo + (dR - d1[k]);
-          const double fad = mu1 * (lo - L2[k]);
-          const double flim = fct_limit_sel(A2[k], N3[k] - N4[k], N2[k] - N3[k], ln - N2[k]);
-          outv[k] = N3[k] - (flim - F3[k]);
-          V1[k] = Vx[k];
-          S1[k] = S[k];
-          f1[k] = fR;
-          d1[k] = dR;
-          L2[k] = lo;
-          N4[k] = N3[k];
-          N3[k] = N2[k];
-          N2[k] = ln;
-          A2[k] = fad;
-          F3[k] = flim;
+        for (int j = 0; j < 3; ++j) {
+          const bool has_src = (half == 1) || (j == 2);  // pz and Q1..Q3 carry z-sources
+          const double fR = 0.5 * e * (zp.V1[j] + Vx[j]);
+          const double dR = nu * (Vx[j] - zp.V1[j]);
+          const double lo = has_src ? zp.V1[j] + dt * zp.S1[j] - (fR - zp.f1[j]) : zp.V1[j] - (fR - zp.f1[j]);
+          const double ln = lo + (dR - zp.d1[j]);
+          const double fad = zp.mu1 * (lo - zp.L2[j]);
+          const double flim = fct_limit_sel(zp.A2[j], zp.N3[j] - zp.N4[j], zp.N2[j] - zp.N3[j], ln - zp.N2[j]);
+          outv[j] = zp.N3[j] - (flim - zp.F3[j]);
+          zp.V1[j] = Vx[j];
+          zp.S1[j] = S[j];
+          zp.f1[j] = fR;
+          zp.d1[j] = dR;
+          zp.L2[j] = lo;
+          zp.N4[j] = zp.N3[j];
+          zp.N3[j] = zp.N2[j];
+          zp.N2[j] = ln;
+          zp.A2[j] = fad;
+          zp.F3[j] = flim;
         }
-        U1 = vz;
-        mu1 = mu;
+        zp.U1 = vz;
+        zp.mu1 = mu;
         const int o = r - 3;
         if (owner && o >= zs && o < ze) {
           // YM_Fluid.cu:20-29 (density floor, wall momentum)
-          if (outv[FN] < 0.05) outv[FN] = 0.05;
-          if (wall && (x_own == 0 || x_own == nx - 1)) outv[FPX] = 0.0;
+          if (half == 0) {
+            if (outv[0] < 0.05) outv[0] = 0.05;
+            if (wall && (x_own == 0 || x_own == nx - 1)) outv[1] = 0.0;
+          }
           double* const* dst = beam ? out.b : out.a;
           const size_t gi = idx2(x_own, o, nx);
 #pragma unroll
-          for (int k = 0; k < 6; ++k) dst[k][gi] = outv[k];
+          for (int j = 0; j < 3; ++j) dst[k0 + j][gi] = outv[j];
         }
       }
     }
@@ -392,11 +413,11 @@ static cudaError_t launch_fct_t(const State& in, const State& out, const StepPar
   sc.bulk = (allow_bulk && p.periodic_x && (p.nx % 2) == 0 && p.nx >= TB + 2) ? 1 : 0;
   sc.err = err;
   const int grid = std::min(sc.nitems, grid_ctas);
-  fct_fused_kernel<TB, NST><<<grid, 2 * TB, fct_smem_bytes<TB>(NST), s>>>(in, out, p, sc);
+  fct_fused_kernel<TB, NST><<<grid, 4 * TB, fct_smem_bytes<TB>(NST), s>>>(in, out, p, sc);
   return cudaGetLastError();
 }
 
-constexpr int FCT_NST = 3;
+constexpr int FCT_NST = 4;
 
 cudaError_t prepare_fct(int tb) {
   switch (tb) {
@@ -410,9 +431,9 @@ cudaError_t prepare_fct(int tb) {
 int fct_ctas_per_sm(int tb) {
   int n = 0;
   switch (tb) {
-    case 32: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fct_fused_kernel<32, FCT_NST>, 64, fct_smem_bytes<32>(FCT_NST)); break;
-    case 64: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fct_fused_kernel<64, FCT_NST>, 128, fct_smem_bytes<64>(FCT_NST)); break;
-    case 128: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fct_fused_kernel<128, FCT_NST>, 256, fct_smem_bytes<128>(FCT_NST)); break;
+    case 32: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fct_fused_kernel<32, FCT_NST>, 128, fct_smem_bytes<32>(FCT_NST)); break;
+    case 64: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fct_fused_kernel<64, FCT_NST>, 256, fct_smem_bytes<64>(FCT_NST)); break;
+    case 128: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fct_fused_kernel<128, FCT_NST>, 512, fct_smem_bytes<128>(FCT_NST)); break;
     default: break;
   }
   return n;

@@ -144,8 +144,10 @@ __global__ void __launch_bounds__(MX_NT, 3)
     for (int q = q_first; q <= q_last; ++q) {
       const int s = (int)(consumed % NST);
       const int sprev = (int)((consumed + NST - 1) % NST);
-      if (bulk)
-        mbar_wait(&bars[s], (consumed / NST) & 1u, sc.err);
+      if (bulk) {  // one thread polls the stage's mbarrier; the CTA barrier below
+        // releases the others after it (no spinning by every thread)
+        if (tid == 0) mbar_wait(&bars[s], (consumed / NST) & 1u, sc.err);
+      }
       else
         cp_async_wait<NST - 3>();
       __syncthreads();  // row q staged by every thread; row q-2's stage is free
