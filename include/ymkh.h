@@ -185,6 +185,24 @@ int ymkh_destroy(ymkh_ctx* ctx);
  * cos_out/sin_out are host arrays of (m_hi-m_lo+1)*nz floats, mode-major. */
 int ymkh_twiddles(int nz, int m_lo, int m_hi, float* cos_out, float* sin_out);
 
+/* Batches (no reference counterpart; the reference runs one configuration
+ * per process, ymgpu2d/scripts/*.sh).  Bound runs of any grid sizes and
+ * parameters advance together: each step launches one FCT and one Maxwell
+ * kernel over the (run, strip, segment) items of all members, then the
+ * per-run filter stages.  A run's state after k batch steps is bit-identical
+ * to k ymkh_step calls on it alone.  Membership may change between calls
+ * (continuous batching); a run belongs to at most one batch at a time and
+ * must not be stepped alone while it is a member. */
+typedef struct ymkh_batch ymkh_batch;
+int ymkh_batch_create(ymkh_batch** out);
+int ymkh_batch_add(ymkh_batch* batch, ymkh_ctx* run);
+int ymkh_batch_remove(ymkh_batch* batch, ymkh_ctx* run);
+int ymkh_batch_size(ymkh_batch* batch);
+int ymkh_batch_set_graph_steps(ymkh_batch* batch, int nsteps_per_graph);
+int ymkh_batch_step(ymkh_batch* batch, int nsteps, void* stream);
+int ymkh_batch_check(ymkh_batch* batch, void* stream);
+int ymkh_batch_destroy(ymkh_batch* batch);
+
 /* Number of kernel launches issued by this library since load (all entry
  * points, all threads).  Used to report launch counts. */
 long long ymkh_launch_count(void);

@@ -82,6 +82,14 @@ _SIGS = {
     "ymkh_mode_amp": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_void_p]),
     "ymkh_destroy": (C.c_int, [C.c_void_p]),
     "ymkh_check": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ymkh_batch_create": (C.c_int, [C.POINTER(C.c_void_p)]),
+    "ymkh_batch_add": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ymkh_batch_remove": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ymkh_batch_size": (C.c_int, [C.c_void_p]),
+    "ymkh_batch_set_graph_steps": (C.c_int, [C.c_void_p, C.c_int]),
+    "ymkh_batch_step": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "ymkh_batch_check": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ymkh_batch_destroy": (C.c_int, [C.c_void_p]),
     "ymkh_twiddles": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "ymkh_launch_count": (C.c_longlong, []),
     "ymkh_stage_times": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_float), C.c_int]),

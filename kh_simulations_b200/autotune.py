@@ -1,0 +1,100 @@
+"""Per grid-size-class launch-shape autotuner.
+
+For a grid-size class (NZ and NX rounded to powers of two, band filter on or
+off) it times the fused FCT kernel for each candidate strip width (the tile
+shape: 32, 64 or 128 x-sweep positions per beam) and z-segment length
+(rows per work item, which sets how often the 3-row z halo is re-swept),
+then the number of steps per captured CUDA graph, and keeps the fastest.
+Results are cached in a JSON table (``tuned.json`` beside this module, or
+the path in ``KH_TUNING_FILE``) that ``KHRun(tune=True)`` consults.
+
+The reference has no tuner: its launch shapes are fixed
+(ymgpu2d/main_ym.cu:220-221, YM_FCT.cu:34-35, 60-63).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import math
+import os
+from pathlib import Path
+
+from . import _lib
+
+TABLE = Path(os.environ.get("KH_TUNING_FILE", Path(__file__).with_name("tuned.json")))
+
+
+def size_class(nx: int, nz: int, filtered: bool) -> str:
+    return f"nx{2 ** round(math.log2(max(nx, 1)))}_nz{2 ** round(math.log2(max(nz, 1)))}_{'f' if filtered else 'n'}"
+
+
+def load_table() -> dict:
+    try:
+        return json.loads(TABLE.read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def lookup(nx: int, nz: int, filtered: bool):
+    return load_table().get(size_class(nx, nz, filtered))
+
+
+def candidates(nx: int, nz: int):
+    tbs = [tb for tb in (32, 64, 128) if nx >= tb - 6]
+    segs = sorted({s for s in (32, 64, 128, 256, 512) if s <= max(32, nz)})
+    return [(tb, s) for tb in tbs for s in segs]
+
+
+def tune(run, reps: int = 3, graph_candidates=(2, 4, 8), save: bool = True) -> dict:
+    """Time the candidates on `run` (a KHRun, state initialised) and record
+    the best shape for its size class."""
+    import torch
+
+    lib = _lib.load()
+    stream = torch.cuda.Stream(device=run.device)
+    out = (C.c_float * 8)()
+    best = None
+    timings = {}
+    for tb, seg in candidates(run.d.nx, run.d.nz):
+        _lib.check(lib.ymkh_set_fct_shape(run.ctx, tb, seg), "ymkh_set_fct_shape")
+        _lib.check(lib.ymkh_stage_times(run.ctx, 1, C.c_void_p(stream.cuda_stream), out, 8), "warm-up")
+        _lib.check(lib.ymkh_stage_times(run.ctx, reps, C.c_void_p(stream.cuda_stream), out, 8), "stage times")
+        ms = out[0] / reps
+        timings[f"{tb}x{seg}"] = ms
+        if best is None or ms < best[0]:
+            best = (ms, tb, seg)
+    _, tb, seg = best
+    _lib.check(lib.ymkh_set_fct_shape(run.ctx, tb, seg), "ymkh_set_fct_shape")
+    gbest = None
+    for g in graph_candidates:
+        _lib.check(lib.ymkh_set_graph_steps(run.ctx, g), "ymkh_set_graph_steps")
+        n = 4 * g
+        run.step(n, stream)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run.step(n, stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / n
+        if gbest is None or ms < gbest[0]:
+            gbest = (ms, g)
+    _lib.check(lib.ymkh_set_graph_steps(run.ctx, gbest[1]), "ymkh_set_graph_steps")
+    entry = {"fct_strip": tb, "fct_segment": seg, "graph_steps": gbest[1], "fct_ms": best[0],
+             "step_ms": gbest[0], "fct_candidates_ms": timings}
+    if save:
+        table = load_table()
+        table[size_class(run.d.nx, run.d.nz, bool(run.d.bands))] = entry
+        TABLE.write_text(json.dumps(table, indent=1, sort_keys=True))
+    return entry
+
+
+def apply(run) -> bool:
+    """Apply a cached shape for the run's size class; False if none."""
+    e = lookup(run.d.nx, run.d.nz, bool(run.d.bands))
+    if not e:
+        return False
+    lib = _lib.load()
+    _lib.check(lib.ymkh_set_fct_shape(run.ctx, int(e["fct_strip"]), int(e["fct_segment"])), "ymkh_set_fct_shape")
+    _lib.check(lib.ymkh_set_graph_steps(run.ctx, int(e["graph_steps"])), "ymkh_set_graph_steps")
+    return True

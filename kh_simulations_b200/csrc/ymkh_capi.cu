@@ -76,6 +76,9 @@ struct ymkh_ctx {
   int sms = 148;
   bool aligned16 = false;   // every bound array 16-byte aligned: TMA bulk row copies allowed
   unsigned* derr = nullptr; // device error word of the bounded in-kernel waits
+  RunDesc* ddesc = nullptr; // device run descriptors for start buffer 0 and 1
+  int fct_items = 0, mx_items = 0;
+  bool desc_ok = false;
   // CUDA graphs of `graph_steps` steps, one per starting buffer
   int graph_steps = 4;
   cudaGraphExec_t gexec[2]{nullptr, nullptr};
@@ -172,12 +175,43 @@ void choose_launch_shape(ymkh_ctx* c) {
   c->fct_tx = c->nx >= 128 ? 64 : 32;
   const int fct_per_sm = std::max(1, fct_ctas_per_sm(c->fct_tx));
   c->fct_grid = c->sms * fct_per_sm;
-  const int fstrips = (c->nx + (c->fct_tx - 6) - 1) / (c->fct_tx - 6);
+  const int fstrips = fct_nstrips(c->nx, c->fct_tx);
   c->fct_seg = pick_segment(c->nz, fstrips, c->fct_grid);
   const int mx_per_sm = std::max(1, maxwell_ctas_per_sm());
   c->mx_grid = c->sms * mx_per_sm;
-  const int mw = maxwell_strip_width();
-  c->mx_seg = pick_segment(c->nz, (c->nx + mw - 1) / mw, c->mx_grid);
+  c->mx_seg = pick_segment(c->nz, maxwell_nstrips(c->nx), c->mx_grid);
+}
+
+RunDesc make_desc(const ymkh_ctx* c, int start, int tb, int fct_item0, int mx_item0) {
+  RunDesc d{};
+  d.in = c->buf[start];
+  d.out = c->buf[1 - start];
+  d.p = c->sp;
+  d.fct_nstrips = fct_nstrips(c->nx, tb);
+  d.fct_seg = c->fct_seg;
+  d.fct_item0 = fct_item0;
+  d.fct_bulk = (c->aligned16 && fct_bulk_ok(c->sp, tb)) ? 1 : 0;
+  d.mx_nstrips = maxwell_nstrips(c->nx);
+  d.mx_seg = c->mx_seg;
+  d.mx_item0 = mx_item0;
+  d.mx_bulk = (c->aligned16 && maxwell_bulk_ok(c->sp)) ? 1 : 0;
+  return d;
+}
+
+int items_fct(const RunDesc& d, int nz) { return d.fct_nstrips * ((nz + d.fct_seg - 1) / d.fct_seg); }
+int items_mx(const RunDesc& d, int nz) { return d.mx_nstrips * ((nz + d.mx_seg - 1) / d.mx_seg); }
+
+// Device descriptors of this run for both start buffers (single-run tables).
+int upload_desc(ymkh_ctx* c) {
+  c->desc_ok = false;
+  if (!c->bound) return 0;
+  if (!c->ddesc) CK(cudaMalloc(&c->ddesc, 2 * sizeof(RunDesc)), "cudaMalloc run descriptors");
+  RunDesc h[2] = {make_desc(c, 0, c->fct_tx, 0, 0), make_desc(c, 1, c->fct_tx, 0, 0)};
+  c->fct_items = items_fct(h[0], c->nz);
+  c->mx_items = items_mx(h[0], c->nz);
+  CK(cudaMemcpy(c->ddesc, h, sizeof h, cudaMemcpyHostToDevice), "upload run descriptors");
+  c->desc_ok = true;
+  return 0;
 }
 
 ArrayList list21(const State& s) {
@@ -203,15 +237,9 @@ void mark(ymkh_ctx* c, int stage, cudaStream_t s) {
   if (c->timing) cudaEventRecord(c->ev[stage], s);
 }
 
-int step_once(ymkh_ctx* c, cudaStream_t s) {
-  const State& in = c->buf[c->cur];
-  const State& out = c->buf[1 - c->cur];
-  mark(c, ST_FCT, s);
-  CK(launch_fct(in, out, c->sp, c->fct_tx, c->fct_seg, c->fct_grid, c->aligned16, c->derr, s), "fct_fused_kernel");
-  mark(c, ST_MAXWELL, s);
-  CK(launch_maxwell(out, in, out, c->sp, c->mx_seg, c->mx_grid, c->aligned16, c->derr, s), "maxwell_fused_kernel");
+// Stages after the fused FCT and Maxwell launches, on the run's new buffer.
+int post_stages(ymkh_ctx* c, const State& out, cudaStream_t s) {
   mark(c, ST_POINTWISE, s);
-  g_launches += 2;
   if (c->prm.xi_sponge > 0.0) { CK(launch_sponge_xicut(list12(out), c->sp, 0, s), "sponge"); g_launches++; }
   if (c->prm.xi_cut > 0.0) { CK(launch_sponge_xicut(list12(out), c->sp, 1, s), "xi_cut"); g_launches++; }
   mark(c, ST_ZMEAN, s);
@@ -235,6 +263,20 @@ int step_once(ymkh_ctx* c, cudaStream_t s) {
     CK(cudaMemsetAsync(out.f[EZ1], 0, bytes, s), "zero Ez1");
   }
   mark(c, ST_COUNT, s);
+  return 0;
+}
+
+// One reference iteration from buffer c->cur into buffer 1 - c->cur.
+int step_once(ymkh_ctx* c, cudaStream_t s) {
+  if (!c->desc_ok) { int rc = upload_desc(c); if (rc) return rc; }
+  RunTable T{c->ddesc + c->cur, 1, c->fct_items, c->mx_items, c->derr};
+  mark(c, ST_FCT, s);
+  CK(launch_fct_table(T, c->fct_tx, c->fct_grid, s), "fct_fused_kernel");
+  mark(c, ST_MAXWELL, s);
+  CK(launch_maxwell_table(T, c->mx_grid, s), "maxwell_fused_kernel");
+  g_launches += 2;
+  int rc = post_stages(c, c->buf[1 - c->cur], s);
+  if (rc) return rc;
   c->cur = 1 - c->cur;
   return 0;
 }
@@ -323,7 +365,7 @@ int ymkh_set_params(ymkh_ctx* c, const ymkh_params* p) {
   if (!c || !p) return set_err(YMKH_EINVAL, "null argument");
   int rc = setup_params(c, p);
   if (rc) return rc;
-  return 0;
+  return upload_desc(c);
 }
 
 static State make_state(double* const f[12], double* const a[6], double* const b[6]) {
@@ -366,7 +408,7 @@ int ymkh_bind_state(ymkh_ctx* c, double* const fields[YMKH_NFIELDS], double* con
   c->cur = 0;
   c->bound = true;
   c->aligned16 = aligned16(c->buf[0]) && aligned16(c->buf[1]);
-  return 0;
+  return upload_desc(c);
 }
 
 // Zero-copy form: the caller provides both buffers; after ymkh_step the
@@ -384,7 +426,7 @@ int ymkh_bind_state2(ymkh_ctx* c, double* const* state0, double* const* state1) 
   c->cur = 0;
   c->bound = true;
   c->aligned16 = aligned16(s0) && aligned16(s1);
-  return 0;
+  return upload_desc(c);
 }
 
 // Reads (and clears) the device error word set by in-kernel waits that ran
@@ -483,7 +525,7 @@ int ymkh_set_fct_shape(ymkh_ctx* c, int tx, int seg) {
   c->fct_tx = tx;
   c->fct_seg = seg;
   c->fct_grid = c->sms * std::max(1, fct_ctas_per_sm(tx));
-  return 0;
+  return upload_desc(c);
 }
 
 int ymkh_get_fct_shape(ymkh_ctx* c, int* tx, int* seg) {
@@ -557,6 +599,7 @@ int ymkh_destroy(ymkh_ctx* c) {
   if (c->edev) cudaFree(c->edev);
   if (c->mcol) cudaFree(c->mcol);
   if (c->derr) cudaFree(c->derr);
+  if (c->ddesc) cudaFree(c->ddesc);
   delete c;
   return 0;
 }
@@ -574,6 +617,204 @@ int ymkh_twiddles(int nz, int m_lo, int m_hi, float* cos_out, float* sin_out) {
   cudaFree(dc);
   cudaFree(ds);
   CK(e, "twiddle table");
+  return 0;
+}
+
+// ------------------------------------------------------------------ batches
+// Runs of any sizes advance together: one FCT and one Maxwell launch per step
+// cover the (run, strip, segment) items of every member; the post-Maxwell
+// stages are launched per member.  Steps can be captured as CUDA graphs.
+
+struct ymkh_batch {
+  std::vector<ymkh_ctx*> runs;
+  RunDesc* ddesc = nullptr;  // [2][cap]: tables for the members' current / next buffers
+  int cap = 0;
+  int fct_items = 0, mx_items = 0;
+  int tb = 64, fct_grid = 0, mx_grid = 0;
+  unsigned* derr = nullptr;
+  bool dirty = true;
+  int parity = 0;            // steps taken since the tables were built, mod 2
+  int graph_steps = 4;
+  cudaGraphExec_t gexec = nullptr;
+  cudaStream_t gstream = nullptr;
+  long long glaunches = 0;
+};
+
+namespace {
+
+void batch_drop_graph(ymkh_batch* b) {
+  if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; b->gstream = nullptr; }
+}
+
+int batch_build(ymkh_batch* b) {
+  const int n = (int)b->runs.size();
+  if (n > b->cap) {
+    if (b->ddesc) cudaFree(b->ddesc);
+    b->cap = std::max(n, 2 * b->cap);
+    CK(cudaMalloc(&b->ddesc, 2 * (size_t)b->cap * sizeof(RunDesc)), "cudaMalloc batch descriptors");
+  }
+  std::vector<RunDesc> h(2 * (size_t)std::max(n, 1));
+  int f0 = 0, m0 = 0;
+  for (int i = 0; i < n; ++i) {
+    ymkh_ctx* c = b->runs[i];
+    RunDesc d0 = make_desc(c, c->cur, b->tb, f0, m0);
+    RunDesc d1 = make_desc(c, 1 - c->cur, b->tb, f0, m0);
+    // finer segments than a lone run needs: items of many runs share the GPU
+    d0.fct_seg = d1.fct_seg = std::min(c->nz, 128);
+    d0.mx_seg = d1.mx_seg = std::min(c->nz, 128);
+    d0.fct_item0 = d1.fct_item0 = f0;
+    d0.mx_item0 = d1.mx_item0 = m0;
+    h[i] = d0;
+    h[n + i] = d1;
+    f0 += items_fct(d0, c->nz);
+    m0 += items_mx(d0, c->nz);
+  }
+  b->fct_items = f0;
+  b->mx_items = m0;
+  if (n) {
+    CK(cudaMemcpy(b->ddesc, h.data(), (size_t)n * sizeof(RunDesc), cudaMemcpyHostToDevice), "upload batch table");
+    CK(cudaMemcpy(b->ddesc + b->cap, h.data() + n, (size_t)n * sizeof(RunDesc), cudaMemcpyHostToDevice),
+       "upload batch table");
+  }
+  b->parity = 0;
+  b->dirty = false;
+  batch_drop_graph(b);
+  return 0;
+}
+
+int batch_step_once(ymkh_batch* b, cudaStream_t s) {
+  const int n = (int)b->runs.size();
+  if (!n) return 0;
+  RunTable T{b->ddesc + (size_t)b->parity * b->cap, n, b->fct_items, b->mx_items, b->derr};
+  CK(launch_fct_table(T, b->tb, b->fct_grid, s), "fct_fused_kernel (batch)");
+  CK(launch_maxwell_table(T, b->mx_grid, s), "maxwell_fused_kernel (batch)");
+  g_launches += 2;
+  for (ymkh_ctx* c : b->runs) {
+    int rc = post_stages(c, c->buf[1 - c->cur], s);
+    if (rc) return rc;
+    c->cur = 1 - c->cur;
+  }
+  b->parity ^= 1;
+  return 0;
+}
+
+}  // namespace
+
+int ymkh_batch_create(ymkh_batch** out) {
+  if (!out) return set_err(YMKH_EINVAL, "null argument");
+  ymkh_batch* b = new ymkh_batch();
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  b->fct_grid = sms * std::max(1, fct_ctas_per_sm(b->tb));
+  b->mx_grid = sms * std::max(1, maxwell_ctas_per_sm());
+  if (cudaMalloc(&b->derr, sizeof(unsigned)) != cudaSuccess || cudaMemset(b->derr, 0, sizeof(unsigned)) != cudaSuccess) {
+    delete b;
+    return set_err(YMKH_ENOMEM, "cudaMalloc batch error word");
+  }
+  *out = b;
+  return 0;
+}
+
+int ymkh_batch_add(ymkh_batch* b, ymkh_ctx* c) {
+  if (!b || !c) return set_err(YMKH_EINVAL, "null argument");
+  if (!c->bound) return set_err(YMKH_ESTATE, "run state not bound");
+  for (ymkh_ctx* r : b->runs) if (r == c) return set_err(YMKH_EINVAL, "run already in the batch");
+  b->runs.push_back(c);
+  b->dirty = true;
+  return 0;
+}
+
+int ymkh_batch_remove(ymkh_batch* b, ymkh_ctx* c) {
+  if (!b || !c) return set_err(YMKH_EINVAL, "null argument");
+  auto it = std::find(b->runs.begin(), b->runs.end(), c);
+  if (it == b->runs.end()) return set_err(YMKH_EINVAL, "run not in the batch");
+  b->runs.erase(it);
+  b->dirty = true;
+  return 0;
+}
+
+int ymkh_batch_size(ymkh_batch* b) { return b ? (int)b->runs.size() : -1; }
+
+int ymkh_batch_set_graph_steps(ymkh_batch* b, int n) {
+  if (!b || n < 0 || (n % 2) != 0) return set_err(YMKH_EINVAL, "graph step count must be even and >= 0");
+  batch_drop_graph(b);
+  b->graph_steps = n;
+  return 0;
+}
+
+int ymkh_batch_step(ymkh_batch* b, int nsteps, void* stream) {
+  if (!b) return set_err(YMKH_EINVAL, "null batch");
+  if (nsteps < 0) return set_err(YMKH_EINVAL, "negative step count");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (b->dirty) { int rc = batch_build(b); if (rc) return rc; }
+  int done = 0;
+  const bool graphs = s != nullptr && b->graph_steps >= 2 && !b->runs.empty();
+  if (graphs) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cs);
+    if (cs == cudaStreamCaptureStatusNone) {
+      // the captured graph starts from the tables' first parity
+      if (b->parity != 0 && nsteps - done > b->graph_steps) {
+        int rc = batch_step_once(b, s);
+        if (rc) return rc;
+        ++done;
+      }
+      while (b->parity == 0 && nsteps - done >= b->graph_steps) {
+        if (!b->gexec || b->gstream != s) {
+          batch_drop_graph(b);
+          std::vector<int> cur0;
+          for (ymkh_ctx* c : b->runs) cur0.push_back(c->cur);
+          cudaGraph_t g = nullptr;
+          CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+          const long long l0 = g_launches.load();
+          int rc = 0;
+          for (int k = 0; k < b->graph_steps && !rc; ++k) rc = batch_step_once(b, s);
+          b->glaunches = g_launches.load() - l0;
+          g_launches -= b->glaunches;
+          cudaError_t ec = cudaStreamEndCapture(s, &g);
+          for (size_t i = 0; i < b->runs.size(); ++i) b->runs[i]->cur = cur0[i];  // nothing ran yet
+          b->parity = 0;
+          if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+          CK(ec, "end capture");
+          cudaError_t ei = cudaGraphInstantiate(&b->gexec, g, 0);
+          cudaGraphDestroy(g);
+          CK(ei, "graph instantiate");
+          b->gstream = s;
+        }
+        CK(cudaGraphLaunch(b->gexec, s), "graph launch");
+        g_launches += b->glaunches;
+        done += b->graph_steps;  // even: every member ends in the buffer it started from
+      }
+    }
+  }
+  for (; done < nsteps; ++done) {
+    int rc = batch_step_once(b, s);
+    if (rc) return rc;
+  }
+  for (ymkh_ctx* c : b->runs)
+    if (!c->dual && c->cur == 1) { int rc = copy_back(c, s); if (rc) return rc; }
+  return 0;
+}
+
+int ymkh_batch_check(ymkh_batch* b, void* stream) {
+  if (!b) return set_err(YMKH_EINVAL, "null batch");
+  unsigned h = 0;
+  CK(cudaMemcpyAsync(&h, b->derr, sizeof h, cudaMemcpyDeviceToHost, (cudaStream_t)stream), "error word D2H");
+  CK(cudaStreamSynchronize((cudaStream_t)stream), "error word sync");
+  if (h) {
+    cudaMemsetAsync(b->derr, 0, sizeof(unsigned), (cudaStream_t)stream);
+    return set_err(YMKH_ECUDA, "a bounded in-kernel wait timed out (error word %u)", h);
+  }
+  return 0;
+}
+
+int ymkh_batch_destroy(ymkh_batch* b) {
+  if (!b) return 0;
+  batch_drop_graph(b);
+  if (b->ddesc) cudaFree(b->ddesc);
+  if (b->derr) cudaFree(b->derr);
+  delete b;
   return 0;
 }
 

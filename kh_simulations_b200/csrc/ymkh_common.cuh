@@ -110,13 +110,9 @@ struct InitArgs {
 // outside any stream capture.
 cudaError_t prepare_fct(int tb);
 int fct_ctas_per_sm(int tb);
-cudaError_t launch_fct(const State& in, const State& out, const StepParams& p, int tb, int seg_len, int grid_ctas,
-                       bool allow_bulk, unsigned* err, cudaStream_t s);
 cudaError_t prepare_maxwell();
 int maxwell_ctas_per_sm();
 int maxwell_strip_width();
-cudaError_t launch_maxwell(const State& fluid_new, const State& fields_old, const State& out, const StepParams& p,
-                           int seg_len, int grid_ctas, bool allow_bulk, unsigned* err, cudaStream_t s);
 cudaError_t launch_sponge_xicut(const ArrayList& a12, const StepParams& p, int cut, cudaStream_t s);
 cudaError_t prepare_column(int nz);
 cudaError_t launch_zmean(const ArrayList& a15, int nx, int nz, cudaStream_t s);
@@ -183,5 +179,53 @@ __device__ __forceinline__ void bulk_row_periodic(double* dst, const double* row
     x = 0;
   }
 }
+
+}  // namespace ymkh
+
+namespace ymkh {
+
+// One run of a batch as the fused kernels see it: its start-of-step and
+// next-step buffers, its step parameters and its (strip, segment) schedules.
+// Items of run i occupy [item0, item0 + nstrips * nsegments) of the batch's
+// flattened work lists.
+struct RunDesc {
+  State in;
+  State out;
+  StepParams p;
+  int fct_nstrips, fct_seg, fct_item0, fct_bulk;
+  int mx_nstrips, mx_seg, mx_item0, mx_bulk;
+};
+
+struct RunTable {
+  const RunDesc* runs;  // device array, item0 ascending
+  int nruns;
+  int fct_items, mx_items;
+  unsigned* err;  // device error word of the bounded in-kernel waits
+};
+
+// Index of the run owning flattened item g (binary search on item0).
+__device__ __forceinline__ int find_run(const RunDesc* runs, int nruns, int g, bool maxwell) {
+  int lo = 0, hi = nruns - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    const int i0 = maxwell ? runs[mid].mx_item0 : runs[mid].fct_item0;
+    if (i0 <= g) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Cooperative copy of a run descriptor into shared memory (8-byte words).
+__device__ __forceinline__ void load_desc(RunDesc* dst, const RunDesc* src) {
+  const unsigned long long* s = reinterpret_cast<const unsigned long long*>(src);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(RunDesc) / 8); i += blockDim.x) d[i] = s[i];
+}
+
+cudaError_t launch_fct_table(const RunTable& T, int tb, int grid_ctas, cudaStream_t s);
+cudaError_t launch_maxwell_table(const RunTable& T, int grid_ctas, cudaStream_t s);
+int fct_nstrips(int nx, int tb);
+int maxwell_nstrips(int nx);
+int fct_bulk_ok(const StepParams& p, int tb);
+int maxwell_bulk_ok(const StepParams& p);
 
 }  // namespace ymkh

@@ -78,13 +78,6 @@ constexpr size_t fct_smem_bytes(int nst) {
          (size_t)8 * nst + 16;
 }
 
-struct FctSched {
-  int nstrips;   // strips of TB-6 output columns
-  int seg_len;   // rows per z-segment
-  int nitems;    // nstrips * nsegments
-  int bulk;      // 1: TMA bulk row copies (periodic x, even NX >= TB+2)
-  unsigned* err; // device error word (bounded waits that ran out)
-};
 
 // Per-thread z-pipeline state for the three swept variables of one half
 // (H = 0: n, px, pz; H = 1: Q1, Q2, Q3) of one beam.
@@ -95,8 +88,7 @@ struct ZPipe {
 
 template <int TB, int NST>
 __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
-    fct_fused_kernel(const __grid_constant__ State st, const __grid_constant__ State out,
-                     const __grid_constant__ StepParams p, const FctSched sc) {
+    fct_fused_kernel(const __grid_constant__ RunTable T) {
   constexpr int W = TB + 2;
   constexpr int NT = 4 * TB;
   constexpr int TO = TB - 6;  // output columns per strip
@@ -107,36 +99,46 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
   uint64_t* const bars = reinterpret_cast<uint64_t*>(
       (reinterpret_cast<uintptr_t>(xtab + W) + 15) & ~static_cast<uintptr_t>(15));
 
-  const int nx = p.nx, nz = p.nz;
+  __shared__ RunDesc rd;
+  __shared__ int s_run;
+  const State& st = rd.in;
+  const State& out = rd.out;
+  const StepParams& p = rd.p;
   const int tid = threadIdx.x;
   const int grp = tid / TB;     // (beam, half) group, 0..3
   const int beam = grp >> 1;
   const int half = grp & 1;     // 0: n, px, pz   1: Q1, Q2, Q3
   const int t = tid - grp * TB;
   const int sp = t + 1;         // this thread's stage position
-  const bool warm = p.warm_T > 0.0;
-  const bool wall = !p.periodic_x;
-  const bool bulk = sc.bulk != 0;
-  const double dt = p.dt;
-  const double dtdx = p.dt / p.dx;
-  const double dtdz = p.dt / p.dz;
   double* const wb = wk + (size_t)beam * WB_SIZE * W;
   const int k0 = 3 * half;      // first swept variable of this half
 
-  if (bulk && tid == 0) {
+  if (tid == 0) {
     for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  __syncthreads();
   unsigned issued = 0, consumed = 0;  // rows issued / consumed by this CTA (all items)
+  unsigned phase_bits = 0;            // per-stage mbarrier phase of the bulk path
 
-  for (int item = blockIdx.x; item < sc.nitems; item += gridDim.x) {
-    const int strip = item % sc.nstrips;
-    const int x0 = strip * TO;
-    const int zs = (item / sc.nstrips) * sc.seg_len;
-    const int ze = min(nz, zs + sc.seg_len);
-
+  for (int item = blockIdx.x; item < T.fct_items; item += gridDim.x) {
     __syncthreads();  // previous item fully consumed
+    if (tid == 0) s_run = find_run(T.runs, T.nruns, item, false);
+    __syncthreads();
+    load_desc(&rd, &T.runs[s_run]);
+    __syncthreads();
+    const int nx = p.nx, nz = p.nz;
+    const bool warm = p.warm_T > 0.0;
+    const bool wall = !p.periodic_x;
+    const bool bulk = rd.fct_bulk != 0;
+    const double dt = p.dt;
+    const double dtdx = p.dt / p.dx;
+    const double dtdz = p.dt / p.dz;
+    const int local = item - rd.fct_item0;
+    const int strip = local % rd.fct_nstrips;
+    const int x0 = strip * TO;
+    const int zs = (local / rd.fct_nstrips) * rd.fct_seg;
+    const int ze = min(nz, zs + rd.fct_seg);
+
     if (!bulk)
       for (int i = tid; i < W; i += NT) xtab[i] = xmap(x0 - 4 + i, nx, p.periodic_x);
     __syncthreads();
@@ -221,7 +223,8 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
       const int s = (int)(consumed % NST);
       if (bulk) {  // one thread polls the stage's mbarrier; the CTA barrier below
         // releases the others after it (no spinning by every thread)
-        if (tid == 0) mbar_wait(&bars[s], (consumed / NST) & 1u, sc.err);
+        if (tid == 0) mbar_wait(&bars[s], (phase_bits >> s) & 1u, T.err);
+        phase_bits ^= 1u << s;
       } else {
         cp_async_wait<NST - 2>();
       }
@@ -399,25 +402,26 @@ static cudaError_t prepare_fct_t() {
                               (int)fct_smem_bytes<TB>(NST));
 }
 
+constexpr int FCT_NST = 4;
+
+int fct_nstrips(int nx, int tb) { return (nx + (tb - 6) - 1) / (tb - 6); }
+
+int fct_bulk_ok(const StepParams& p, int tb) { return (p.periodic_x && (p.nx % 2) == 0 && p.nx >= tb + 2) ? 1 : 0; }
+
 // The kernel reads start-of-step values across strip and segment halos while
-// other CTAs write theirs, so the fluid it writes goes to a second state
-// buffer (`out`); fields are only read.  grid_ctas persistent CTAs take the
-// (strip, segment) items round-robin.
-template <int TB, int NST>
-static cudaError_t launch_fct_t(const State& in, const State& out, const StepParams& p, int seg_len, int grid_ctas,
-                                bool allow_bulk, unsigned* err, cudaStream_t s) {
-  FctSched sc;
-  sc.nstrips = (p.nx + (TB - 6) - 1) / (TB - 6);
-  sc.seg_len = seg_len;
-  sc.nitems = sc.nstrips * ((p.nz + seg_len - 1) / seg_len);
-  sc.bulk = (allow_bulk && p.periodic_x && (p.nx % 2) == 0 && p.nx >= TB + 2) ? 1 : 0;
-  sc.err = err;
-  const int grid = std::min(sc.nitems, grid_ctas);
-  fct_fused_kernel<TB, NST><<<grid, 4 * TB, fct_smem_bytes<TB>(NST), s>>>(in, out, p, sc);
+// other CTAs write theirs, so each run's fluid goes to its second buffer
+// (`out`); fields are only read.  grid_ctas persistent CTAs take the
+// flattened (run, strip, segment) items round-robin.
+cudaError_t launch_fct_table(const RunTable& T, int tb, int grid_ctas, cudaStream_t s) {
+  const int grid = std::max(1, std::min(T.fct_items, grid_ctas));
+  switch (tb) {
+    case 32: fct_fused_kernel<32, FCT_NST><<<grid, 128, fct_smem_bytes<32>(FCT_NST), s>>>(T); break;
+    case 64: fct_fused_kernel<64, FCT_NST><<<grid, 256, fct_smem_bytes<64>(FCT_NST), s>>>(T); break;
+    case 128: fct_fused_kernel<128, FCT_NST><<<grid, 512, fct_smem_bytes<128>(FCT_NST), s>>>(T); break;
+    default: return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
-
-constexpr int FCT_NST = 4;
 
 cudaError_t prepare_fct(int tb) {
   switch (tb) {
@@ -437,16 +441,6 @@ int fct_ctas_per_sm(int tb) {
     default: break;
   }
   return n;
-}
-
-cudaError_t launch_fct(const State& in, const State& out, const StepParams& p, int tb, int seg_len, int grid_ctas,
-                       bool allow_bulk, unsigned* err, cudaStream_t s) {
-  switch (tb) {
-    case 32: return launch_fct_t<32, FCT_NST>(in, out, p, seg_len, grid_ctas, allow_bulk, err, s);
-    case 64: return launch_fct_t<64, FCT_NST>(in, out, p, seg_len, grid_ctas, allow_bulk, err, s);
-    case 128: return launch_fct_t<128, FCT_NST>(in, out, p, seg_len, grid_ctas, allow_bulk, err, s);
-    default: return cudaErrorInvalidValue;
-  }
 }
 
 }  // namespace ymkh

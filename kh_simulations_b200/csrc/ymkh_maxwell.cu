@@ -51,14 +51,8 @@ constexpr size_t maxwell_smem_bytes() {
          (size_t)8 * MX_NST + 16;
 }
 
-struct MxSched {
-  int nstrips, seg_len, nitems, bulk;
-  unsigned* err;
-};
-
 __global__ void __launch_bounds__(MX_NT, 3)
-    maxwell_fused_kernel(const __grid_constant__ State fluid_new, const __grid_constant__ State fields_old,
-                         const __grid_constant__ State out, const __grid_constant__ StepParams p, const MxSched sc) {
+    maxwell_fused_kernel(const __grid_constant__ RunTable T) {
   constexpr int TX = MX_TX, W = MX_W, NST = MX_NST, NT = MX_NT;
   extern __shared__ __align__(16) double smem[];
   double* const stage = smem;
@@ -67,28 +61,41 @@ __global__ void __launch_bounds__(MX_NT, 3)
   uint64_t* const bars = reinterpret_cast<uint64_t*>(
       (reinterpret_cast<uintptr_t>(xtab + W) + 15) & ~static_cast<uintptr_t>(15));
 
-  const int nx = p.nx, nz = p.nz;
+  __shared__ RunDesc rd;
+  __shared__ int s_run;
+  // Reads the new fluid (the run's `out` fluid, written by the FCT) and the
+  // start-of-step fields (`in`), writes the new fields to `out`.
+  const State& fluid_new = rd.out;
+  const State& fields_old = rd.in;
+  const State& out = rd.out;
+  const StepParams& p = rd.p;
   const int tid = threadIdx.x;
-  const bool wall = !p.periodic_x;
-  const bool bulk = sc.bulk != 0;
-  const double dt = p.dt, c2 = p.c2, al = p.alpha, e0 = p.eps0;
-  // c = eps_0 = 1 (ymgpu2d/main_ym.cu:69): 1*x and x/1 are exact, so the
-  // products and quotients by them can be skipped without changing a bit
-  const bool unit = (c2 == 1.0 && e0 == 1.0);
 
-  if (bulk && tid == 0) {
+  if (tid == 0) {
     for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  __syncthreads();
   unsigned issued = 0, consumed = 0;
+  unsigned phase_bits = 0;  // per-stage mbarrier phase of the bulk path
 
-  for (int item = blockIdx.x; item < sc.nitems; item += gridDim.x) {
-    const int x0 = (item % sc.nstrips) * TX;
-    const int zs = (item / sc.nstrips) * sc.seg_len;
-    const int ze = min(nz, zs + sc.seg_len);
-
+  for (int item = blockIdx.x; item < T.mx_items; item += gridDim.x) {
     __syncthreads();
+    if (tid == 0) s_run = find_run(T.runs, T.nruns, item, true);
+    __syncthreads();
+    load_desc(&rd, &T.runs[s_run]);
+    __syncthreads();
+    const int nx = p.nx, nz = p.nz;
+    const bool wall = !p.periodic_x;
+    const bool bulk = rd.mx_bulk != 0;
+    const double dt = p.dt, c2 = p.c2, al = p.alpha, e0 = p.eps0;
+    // c = eps_0 = 1 (ymgpu2d/main_ym.cu:69): 1*x and x/1 are exact, so the
+    // products and quotients by them can be skipped without changing a bit
+    const bool unit = (c2 == 1.0 && e0 == 1.0);
+    const int local = item - rd.mx_item0;
+    const int x0 = (local % rd.mx_nstrips) * TX;
+    const int zs = (local / rd.mx_nstrips) * rd.mx_seg;
+    const int ze = min(nz, zs + rd.mx_seg);
+
     for (int i = tid; i < W; i += NT) xtab[i] = xmap(x0 - 2 + i, nx, p.periodic_x);
     __syncthreads();
 
@@ -146,7 +153,8 @@ __global__ void __launch_bounds__(MX_NT, 3)
       const int sprev = (int)((consumed + NST - 1) % NST);
       if (bulk) {  // one thread polls the stage's mbarrier; the CTA barrier below
         // releases the others after it (no spinning by every thread)
-        if (tid == 0) mbar_wait(&bars[s], (consumed / NST) & 1u, sc.err);
+        if (tid == 0) mbar_wait(&bars[s], (phase_bits >> s) & 1u, T.err);
+        phase_bits ^= 1u << s;
       }
       else
         cp_async_wait<NST - 3>();
@@ -273,16 +281,13 @@ int maxwell_ctas_per_sm() {
 
 int maxwell_strip_width() { return MX_TX; }
 
-cudaError_t launch_maxwell(const State& fluid_new, const State& fields_old, const State& out, const StepParams& p,
-                           int seg_len, int grid_ctas, bool allow_bulk, unsigned* err, cudaStream_t s) {
-  MxSched sc;
-  sc.nstrips = (p.nx + MX_TX - 1) / MX_TX;
-  sc.seg_len = seg_len;
-  sc.nitems = sc.nstrips * ((p.nz + seg_len - 1) / seg_len);
-  sc.bulk = (allow_bulk && p.periodic_x && (p.nx % 2) == 0 && p.nx >= MX_W) ? 1 : 0;
-  sc.err = err;
-  const int grid = std::min(sc.nitems, grid_ctas);
-  maxwell_fused_kernel<<<grid, MX_NT, maxwell_smem_bytes(), s>>>(fluid_new, fields_old, out, p, sc);
+int maxwell_nstrips(int nx) { return (nx + MX_TX - 1) / MX_TX; }
+
+int maxwell_bulk_ok(const StepParams& p) { return (p.periodic_x && (p.nx % 2) == 0 && p.nx >= MX_W) ? 1 : 0; }
+
+cudaError_t launch_maxwell_table(const RunTable& T, int grid_ctas, cudaStream_t s) {
+  const int grid = std::max(1, std::min(T.mx_items, grid_ctas));
+  maxwell_fused_kernel<<<grid, MX_NT, maxwell_smem_bytes(), s>>>(T);
   return cudaGetLastError();
 }
 

@@ -59,7 +59,7 @@ class KHRun:
     """One run.  ``state`` is a [24, NZ, NX] float64 CUDA tensor (include/ymkh.h order)."""
 
     def __init__(self, cfg: RunConfig, device: int | str | torch.device = "cuda", *, graph_steps: int | None = None,
-                 fct_shape: tuple | None = None):
+                 fct_shape: tuple | None = None, tune: bool = False):
         if not torch.cuda.is_available():
             raise _lib.YMKHError("KHRun needs a CUDA device (no CPU fallback)")
         self.cfg = cfg
@@ -81,6 +81,10 @@ class KHRun:
                 check(self.lib.ymkh_set_graph_steps(self.ctx, graph_steps), "ymkh_set_graph_steps")
             if fct_shape is not None:
                 check(self.lib.ymkh_set_fct_shape(self.ctx, *fct_shape), "ymkh_set_fct_shape")
+            elif tune:
+                from . import autotune
+
+                autotune.apply(self)
         self.step_count = 0
         self.E0: float | None = None
         self.history: list[EnergyRecord] = []

@@ -1,0 +1,285 @@
+"""``KHServer``: continuous batching of Kelvin–Helmholtz runs.
+
+Requests (an .ini-level ``RunConfig`` plus a step count) arrive over time.
+The server admits them in arrival order while their device footprint fits
+the memory budget, keeps every admitted run's state resident in HBM, and
+advances all admitted runs together through one ``KHBatch`` (one fused FCT
+and one fused Maxwell launch per step over every run's tiles, captured as
+CUDA graphs).  Between step chunks it retires finished runs (freeing their
+memory), halts runs that break the reference's energy rule
+(ymgpu2d/main_ym.cu:249, 467-474) and admits waiting requests: continuous
+batching.  It reports p50/p99 run latency (arrival to completion) and the
+aggregate cell-steps/s; ``serve_sequential`` runs the same requests one by
+one through the plain single-run step for comparison.
+
+The reference has no serving layer: campaigns run one ``ym_coupled``
+process per configuration (ymgpu2d/scripts/*.sh).
+"""
+from __future__ import annotations
+
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .config import RunConfig, derive
+
+BYTES_PER_CELL_STATE = 2 * 24 * 8  # two 24-array FP64 buffers
+
+
+def footprint(cfg: RunConfig) -> int:
+    """Device bytes a run holds while resident: both state buffers, the
+    band-filter twiddles and coefficients, diagnostics (include/ymkh.h)."""
+    d = derive(cfg)
+    cells = d.nx * d.nz
+    fp = BYTES_PER_CELL_STATE * cells
+    if d.bands:
+        maxj = max(2 * (hi - lo + 1) for lo, hi in d.bands)
+        fp += 21 * maxj * d.nx * 8 + sum(2 * (hi - lo + 1) * d.nz * 8 for lo, hi in d.bands)
+    fp += 64 * 1024 + 16 * d.nx
+    return fp
+
+
+@dataclass
+class KHRequest:
+    rid: int
+    cfg: RunConfig
+    steps: int
+    arrival: float = 0.0           # seconds after the server starts
+    admitted: float = math.nan
+    finished: float = math.nan
+    status: str = "pending"        # pending | running | done | halted | rejected
+    energy: float = math.nan
+    state: np.ndarray | None = None
+
+    @property
+    def cells(self) -> int:
+        d = derive(self.cfg)
+        return d.nx * d.nz
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+@dataclass
+class ServeReport:
+    requests: list
+    makespan: float
+    cell_steps: int
+    p50: float
+    p99: float
+    mode: str
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def cell_steps_per_s(self) -> float:
+        return self.cell_steps / self.makespan if self.makespan > 0 else 0.0
+
+    def summary(self) -> dict:
+        n_done = sum(r.status in ("done", "halted") for r in self.requests)
+        return {"mode": self.mode, "requests": len(self.requests), "completed": n_done,
+                "halted": sum(r.status == "halted" for r in self.requests),
+                "rejected": sum(r.status == "rejected" for r in self.requests),
+                "makespan_s": self.makespan, "cell_steps": self.cell_steps,
+                "cell_steps_per_s": self.cell_steps_per_s, "p50_latency_s": self.p50, "p99_latency_s": self.p99,
+                **self.extra}
+
+
+def _percentiles(reqs) -> tuple:
+    lat = [r.latency for r in reqs if r.status in ("done", "halted")]
+    if not lat:
+        return math.nan, math.nan
+    return float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
+
+
+class KHServer:
+    """Continuous-batching server on one GPU.
+
+    budget_bytes: device memory the resident runs may hold together.
+    chunk: steps between admission/retirement decisions.
+    keep_state: copy each finished run's final state to the host.
+    """
+
+    def __init__(self, budget_bytes: int, device="cuda", chunk: int = 100, graph_steps: int = 4,
+                 keep_state: bool = False, check_energy: bool = True, clock=time.perf_counter):
+        self.budget = int(budget_bytes)
+        self.device = device
+        self.chunk = int(chunk)
+        self.graph_steps = graph_steps
+        self.keep_state = keep_state
+        self.check_energy = check_energy
+        self.clock = clock
+
+    # ---------------------------------------------------------------- helpers
+    def _start_run(self, req: KHRequest):
+        from .run import KHRun
+
+        run = KHRun(req.cfg, device=self.device, graph_steps=self.graph_steps)
+        run.init()
+        run.E0 = run.energy()
+        return run
+
+    def _finish(self, req: KHRequest, run, status: str, t: float):
+        req.finished = t
+        req.status = status
+        if self.keep_state:
+            req.state = run.state_numpy()
+        req.energy = run.energy()
+        run.close()
+
+    def admit_order(self, pending: deque, now: float, used: int) -> list:
+        """FIFO admission by footprint: admit the arrived head while it fits;
+        a request larger than the whole budget is rejected."""
+        out = []
+        while pending and pending[0].arrival <= now:
+            req = pending[0]
+            fp = footprint(req.cfg)
+            if fp > self.budget:
+                pending.popleft()
+                req.status = "rejected"
+                continue
+            if used + fp > self.budget:
+                break
+            pending.popleft()
+            used += fp
+            out.append((req, fp))
+        return out
+
+    # ------------------------------------------------------------------ serve
+    def serve(self, requests: list) -> ServeReport:
+        import torch
+
+        from .batch import KHBatch
+
+        stream = torch.cuda.Stream(device=self.device)
+        batch = KHBatch(device=self.device, graph_steps=self.graph_steps)
+        pending = deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
+        active: list = []  # (req, run, fp, remaining)
+        used = 0
+        cell_steps = 0
+        t0 = self.clock()
+        first = pending[0].arrival if pending else 0.0
+        while pending or active:
+            now = self.clock() - t0
+            for req, fp in self.admit_order(pending, now, used):
+                run = self._start_run(req)
+                req.admitted = self.clock() - t0
+                req.status = "running"
+                batch.add(run)
+                active.append([req, run, fp, req.steps])
+                used += fp
+            if not active:
+                if pending:
+                    time.sleep(max(0.0, min(0.05, pending[0].arrival - (self.clock() - t0))))
+                continue
+            k = min(self.chunk, min(a[3] for a in active))
+            batch.step(k, stream)
+            stream.synchronize()
+            for a in active:
+                a[3] -= k
+                cell_steps += k * a[0].cells
+            keep = []
+            for a in active:
+                req, run, fp, rem = a
+                status = None
+                if rem <= 0:
+                    status = "done"
+                elif self.check_energy:
+                    e = run.energy(stream)
+                    if not math.isfinite(e) or e / run.E0 > run.d.energy_thresh:
+                        status = "halted"
+                if status:
+                    batch.remove(run)
+                    self._finish(req, run, status, self.clock() - t0)
+                    used -= fp
+                else:
+                    keep.append(a)
+            active = keep
+        makespan = (self.clock() - t0) - first
+        batch.close()
+        p50, p99 = _percentiles(requests)
+        return ServeReport(requests, makespan, cell_steps, p50, p99, "batched")
+
+    def serve_sequential(self, requests: list) -> ServeReport:
+        """The same requests one by one through the plain single-run step, in
+        arrival order (a request starts when it has arrived and the previous
+        one has finished)."""
+        import torch
+
+        stream = torch.cuda.Stream(device=self.device)
+        order = sorted(requests, key=lambda r: (r.arrival, r.rid))
+        t0 = self.clock()
+        first = order[0].arrival if order else 0.0
+        cell_steps = 0
+        for req in order:
+            if footprint(req.cfg) > self.budget:
+                req.status = "rejected"
+                continue
+            now = self.clock() - t0
+            if req.arrival > now:
+                time.sleep(req.arrival - now)
+            run = self._start_run(req)
+            req.admitted = self.clock() - t0
+            status = "done"
+            left = req.steps
+            while left > 0:
+                k = min(self.chunk, left)
+                run.step(k, stream)
+                left -= k
+                cell_steps += k * req.cells
+                if self.check_energy:
+                    e = run.energy(stream)
+                    if not math.isfinite(e) or e / run.E0 > run.d.energy_thresh:
+                        status = "halted"
+                        break
+            stream.synchronize()
+            self._finish(req, run, status, self.clock() - t0)
+        makespan = (self.clock() - t0) - first
+        p50, p99 = _percentiles(order)
+        return ServeReport(order, makespan, cell_steps, p50, p99, "sequential")
+
+
+def poisson_mix(seed: int, rate: float, duration: float, min_cells: int, max_cells: int, min_steps: int,
+                max_steps: int, base_ini: str, nz_multiple: int = 32) -> list:
+    """Seeded request mix: Poisson arrivals at `rate` per second for
+    `duration` seconds; cell counts log-uniform in [min_cells, max_cells]
+    with NZ:NX = 1:2 (NZ rounded to a multiple of nz_multiple, a power of two
+    when the run suppresses kz=0); V0 ~ U[0.02, 0.2], shear width
+    ~ U[0.5, 2], kz in {0..3}, perturbation ~ U[0.05, 0.2]; kz = 0 suppressed
+    in every other request; steps uniform in [min_steps, max_steps]."""
+    from .config import loads
+
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    rid = 0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration:
+            break
+        cells = math.exp(rng.uniform(math.log(min_cells), math.log(max_cells)))
+        kz0 = rid % 2 == 0
+        nz = math.sqrt(cells / 2.0)
+        if kz0:
+            nz = 2 ** int(round(math.log2(nz)))
+        else:
+            nz = max(nz_multiple, int(round(nz / nz_multiple)) * nz_multiple)
+        nx = 2 * nz
+        v0 = rng.uniform(0.02, 0.2)
+        eps = rng.uniform(0.5, 2.0)
+        kz = int(rng.integers(0, 4))
+        amp = rng.uniform(0.05, 0.2)
+        steps = int(rng.integers(min_steps, max_steps + 1))
+        dz = 2 * math.pi / nz
+        dx = 20.0 / nx
+        # CFL-safe Courant number: dt * sqrt(dx^-2 + dz^-2) <= 0.4 with dt = C dx
+        courant = min(0.4, 0.4 / (dx * math.sqrt(dx ** -2 + dz ** -2)))
+        ini = (base_ini + f"k_mode = {kz}\nV0 = {v0:.6f}\neps_override = {eps:.6f}\nperturb_amp = {amp:.6f}\n"
+               f"nz_override = {nz}\nnx_override = {nx}\ncourant_override = {courant:.6f}\n"
+               f"suppress_kz0 = {1 if kz0 else 0}\n")
+        out.append(KHRequest(rid, loads(ini, f"req{rid}"), steps, t))
+        rid += 1
+    return out

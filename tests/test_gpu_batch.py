@@ -1,0 +1,128 @@
+"""Batched and served forms give the same results as the plain step.
+
+A run advanced inside a batch (one fused FCT and one fused Maxwell launch
+over the tiles of every member) must be bit-identical to the same run
+advanced alone, including when members join and leave between calls
+(continuous batching), and the serving loop's results must equal the same
+requests run one by one."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+MIX = [
+    ("nz_override = 64\nnx_override = 128\nkz_keep_max = 21\n", 0),
+    ("nz_override = 32\nnx_override = 96\nsuppress_kz0 = 1\n", 1),
+    ("nz_override = 128\nnx_override = 256\nhyp_diff = 5e-5\nkz_suppress_hi = 9\n", 2),
+    ("nz_override = 27\nnx_override = 37\n", 3),        # ragged sizes: element load path
+    ("nz_override = 32\nnx_override = 48\nrun_mode = 0\n", 0),  # walls
+]
+
+
+def _cfg(text):
+    from cases import BASE
+    from kh_simulations_b200.config import loads
+
+    return loads(BASE + text)
+
+
+def _alone(text, steps):
+    from kh_simulations_b200.run import KHRun
+
+    r = KHRun(_cfg(text))
+    r.init()
+    r.step(steps)
+    s = r.state_numpy()
+    r.close()
+    return s
+
+
+def test_batch_equals_alone(cuda):
+    import torch
+
+    from kh_simulations_b200.batch import KHBatch
+    from kh_simulations_b200.run import KHRun
+
+    steps = 7
+    runs = []
+    for text, _ in MIX:
+        r = KHRun(_cfg(text))
+        r.init()
+        runs.append(r)
+    b = KHBatch()
+    for r in runs:
+        b.add(r)
+    st = torch.cuda.Stream()
+    b.step(steps, st)  # 3 graph-less steps + one 4-step graph
+    st.synchronize()
+    b.check(st)
+    for (text, _), r in zip(MIX, runs):
+        assert np.array_equal(r.state_numpy(), _alone(text, steps)), text
+    b.close()
+    for r in runs:
+        r.close()
+
+
+def test_continuous_batching_membership_changes(cuda):
+    """Members join and leave between batch calls; every run still ends
+    bit-identical to its solo trajectory."""
+    import torch
+
+    from kh_simulations_b200.batch import KHBatch
+    from kh_simulations_b200.run import KHRun
+
+    st = torch.cuda.Stream()
+    b = KHBatch()
+    r0 = KHRun(_cfg(MIX[0][0]))
+    r0.init()
+    b.add(r0)
+    b.step(5, st)
+    r1 = KHRun(_cfg(MIX[1][0]))
+    r1.init()
+    b.add(r1)
+    b.step(6, st)        # r0: 11, r1: 6
+    b.remove(r0)
+    r2 = KHRun(_cfg(MIX[2][0]))
+    r2.init()
+    b.add(r2)
+    b.step(3, st)        # r1: 9, r2: 3
+    st.synchronize()
+    assert np.array_equal(r0.state_numpy(), _alone(MIX[0][0], 11))
+    assert np.array_equal(r1.state_numpy(), _alone(MIX[1][0], 9))
+    assert np.array_equal(r2.state_numpy(), _alone(MIX[2][0], 3))
+    b.close()
+    for r in (r0, r1, r2):
+        r.close()
+
+
+def test_server_mix_equals_sequential(cuda):
+    from kh_simulations_b200.server import KHRequest, KHServer
+
+    reqs_a = [KHRequest(i, _cfg(t), 20 + 10 * i, arrival=0.01 * i) for i, (t, _) in enumerate(MIX[:4])]
+    reqs_b = [KHRequest(i, _cfg(t), 20 + 10 * i, arrival=0.01 * i) for i, (t, _) in enumerate(MIX[:4])]
+    srv = KHServer(budget_bytes=2 << 30, chunk=8, keep_state=True, check_energy=True)
+    rep_b = srv.serve(reqs_a)
+    rep_s = srv.serve_sequential(reqs_b)
+    for a, s in zip(sorted(reqs_a, key=lambda r: r.rid), sorted(reqs_b, key=lambda r: r.rid)):
+        assert a.status == s.status == "done"
+        assert np.array_equal(a.state, s.state), a.rid
+    assert rep_b.cell_steps == rep_s.cell_steps
+    assert np.isfinite(rep_b.p50) and np.isfinite(rep_b.p99)
+
+
+def test_autotune_runs_and_keeps_results(cuda, tmp_path, monkeypatch):
+    import kh_simulations_b200.autotune as at
+    from kh_simulations_b200.run import KHRun
+
+    monkeypatch.setattr(at, "TABLE", tmp_path / "tuned.json")
+    r = KHRun(_cfg(MIX[2][0]))
+    r.init()
+    e = at.tune(r, reps=1, graph_candidates=(2, 4))
+    assert e["fct_strip"] in (32, 64, 128) and e["graph_steps"] in (2, 4)
+    assert at.lookup(r.d.nx, r.d.nz, True) == e
+    s_tuned = KHRun(_cfg(MIX[2][0]), tune=True)
+    s_tuned.init()
+    s_tuned.step(4)
+    assert np.array_equal(s_tuned.state_numpy(), _alone(MIX[2][0], 4))
+    r.close()
+    s_tuned.close()
