@@ -49,6 +49,12 @@ enum {
   YMKH_ENOMEM = -4    /* allocation failed */
 };
 
+/* Forms of the flux-corrected transport stage (same results bit for bit):
+ * FUSED streams x- and z-sweeps in one pass (fewest bytes, staged rows);
+ * SPLIT runs a coalesced x pass into a 12-array scratch and a coalesced
+ * z pass (more bytes, full-bandwidth access). */
+enum { YMKH_FCT_FUSED = 0, YMKH_FCT_SPLIT = 1 };
+
 /* Filter engines for the periodic-direction DFT mode filter. */
 enum {
   YMKH_FILTER_DFT = 0    /* dense DFT with the reference's FP32-phase twiddles, FP64 sums
@@ -144,6 +150,7 @@ int ymkh_set_current_buffer(ymkh_ctx* ctx, int which);
 int ymkh_set_graph_steps(ymkh_ctx* ctx, int nsteps_per_graph);
 int ymkh_set_fct_shape(ymkh_ctx* ctx, int strip_width, int segment_rows);
 int ymkh_get_fct_shape(ymkh_ctx* ctx, int* strip_width, int* segment_rows);
+int ymkh_set_fct_mode(ymkh_ctx* ctx, int mode);  /* YMKH_FCT_*; chosen per size class by the autotuner */
 
 /* Device time per stage over nsteps uncaptured steps (CUDA events between
  * stages on `stream`), accumulated in out_ms[0..6]: FCT, Maxwell,
@@ -199,6 +206,7 @@ int ymkh_batch_add(ymkh_batch* batch, ymkh_ctx* run);
 int ymkh_batch_remove(ymkh_batch* batch, ymkh_ctx* run);
 int ymkh_batch_size(ymkh_batch* batch);
 int ymkh_batch_set_graph_steps(ymkh_batch* batch, int nsteps_per_graph);
+int ymkh_batch_set_fct_mode(ymkh_batch* batch, int mode);
 int ymkh_batch_step(ymkh_batch* batch, int nsteps, void* stream);
 int ymkh_batch_check(ymkh_batch* batch, void* stream);
 int ymkh_batch_destroy(ymkh_batch* batch);

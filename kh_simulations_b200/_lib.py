@@ -14,6 +14,7 @@ LIB_PATH = _PKG / "libymkh.so"
 NFIELDS, NFLUID, NSTATE = 12, 6, 24
 MAX_EXTRA_BANDS = 4
 FILTER_DFT = 0
+FCT_FUSED, FCT_SPLIT = 0, 1
 
 # state order of include/ymkh.h
 STATE_NAMES = (
@@ -75,6 +76,8 @@ _SIGS = {
     "ymkh_set_graph_steps": (C.c_int, [C.c_void_p, C.c_int]),
     "ymkh_set_fct_shape": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "ymkh_get_fct_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "ymkh_set_fct_mode": (C.c_int, [C.c_void_p, C.c_int]),
+    "ymkh_batch_set_fct_mode": (C.c_int, [C.c_void_p, C.c_int]),
     "ymkh_init": (C.c_int, [C.c_void_p, C.POINTER(InitParams), C.c_void_p]),
     "ymkh_step": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "ymkh_energy": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),

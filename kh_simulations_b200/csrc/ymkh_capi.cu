@@ -77,8 +77,12 @@ struct ymkh_ctx {
   bool aligned16 = false;   // every bound array 16-byte aligned: TMA bulk row copies allowed
   unsigned* derr = nullptr; // device error word of the bounded in-kernel waits
   RunDesc* ddesc = nullptr; // device run descriptors for start buffer 0 and 1
-  int fct_items = 0, mx_items = 0;
+  int fct_items = 0, mx_items = 0, fx_items = 0, fz_items = 0;
   bool desc_ok = false;
+  int fct_mode = YMKH_FCT_SPLIT;  // YMKH_FCT_FUSED or YMKH_FCT_SPLIT
+  double* xscratch = nullptr;     // 12 x-swept fluid arrays of the split form
+  int fz_seg = 128;
+  int fx_grid = 0, fz_grid = 0;
   // CUDA graphs of `graph_steps` steps, one per starting buffer
   int graph_steps = 4;
   cudaGraphExec_t gexec[2]{nullptr, nullptr};
@@ -180,6 +184,8 @@ void choose_launch_shape(ymkh_ctx* c) {
   const int mx_per_sm = std::max(1, maxwell_ctas_per_sm());
   c->mx_grid = c->sms * mx_per_sm;
   c->mx_seg = pick_segment(c->nz, maxwell_nstrips(c->nx), c->mx_grid);
+  c->fx_grid = c->sms * std::max(1, fct_split_ctas_per_sm(0)) * 4;
+  c->fz_grid = c->sms * std::max(1, fct_split_ctas_per_sm(1)) * 4;
 }
 
 RunDesc make_desc(const ymkh_ctx* c, int start, int tb, int fct_item0, int mx_item0) {
@@ -195,7 +201,26 @@ RunDesc make_desc(const ymkh_ctx* c, int start, int tb, int fct_item0, int mx_it
   d.mx_seg = c->mx_seg;
   d.mx_item0 = mx_item0;
   d.mx_bulk = (c->aligned16 && maxwell_bulk_ok(c->sp)) ? 1 : 0;
+  if (c->xscratch)
+    for (int i = 0; i < 6; ++i) {
+      d.xsw.a[i] = c->xscratch + (size_t)i * c->N;
+      d.xsw.b[i] = c->xscratch + (size_t)(6 + i) * c->N;
+    }
+  d.fx_nstrips = fctx_nstrips(c->nx);
+  d.fz_ncols = fctz_ncols(c->nx);
+  d.fz_seg = std::min(c->nz, c->fz_seg);
   return d;
+}
+
+int items_fx(const RunDesc& d, int nz) { return d.fx_nstrips * nz * 2; }
+int items_fz(const RunDesc& d, int nz) { return d.fz_ncols * ((nz + d.fz_seg - 1) / d.fz_seg); }
+
+// The split FCT form needs a 12-array scratch for the x-swept fluid.
+int ensure_xscratch(ymkh_ctx* c) {
+  if (c->fct_mode != YMKH_FCT_SPLIT || c->xscratch) return 0;
+  if (cudaMalloc(&c->xscratch, (size_t)12 * c->N * sizeof(double)) != cudaSuccess)
+    return set_err(YMKH_ENOMEM, "cudaMalloc x-sweep scratch (%zu bytes)", (size_t)12 * c->N * sizeof(double));
+  return 0;
 }
 
 int items_fct(const RunDesc& d, int nz) { return d.fct_nstrips * ((nz + d.fct_seg - 1) / d.fct_seg); }
@@ -206,9 +231,13 @@ int upload_desc(ymkh_ctx* c) {
   c->desc_ok = false;
   if (!c->bound) return 0;
   if (!c->ddesc) CK(cudaMalloc(&c->ddesc, 2 * sizeof(RunDesc)), "cudaMalloc run descriptors");
+  { int rc = ensure_xscratch(c); if (rc) return rc; }
   RunDesc h[2] = {make_desc(c, 0, c->fct_tx, 0, 0), make_desc(c, 1, c->fct_tx, 0, 0)};
+  for (RunDesc& d : h) d.fx_item0 = d.fz_item0 = 0;
   c->fct_items = items_fct(h[0], c->nz);
   c->mx_items = items_mx(h[0], c->nz);
+  c->fx_items = items_fx(h[0], c->nz);
+  c->fz_items = items_fz(h[0], c->nz);
   CK(cudaMemcpy(c->ddesc, h, sizeof h, cudaMemcpyHostToDevice), "upload run descriptors");
   c->desc_ok = true;
   return 0;
@@ -269,9 +298,14 @@ int post_stages(ymkh_ctx* c, const State& out, cudaStream_t s) {
 // One reference iteration from buffer c->cur into buffer 1 - c->cur.
 int step_once(ymkh_ctx* c, cudaStream_t s) {
   if (!c->desc_ok) { int rc = upload_desc(c); if (rc) return rc; }
-  RunTable T{c->ddesc + c->cur, 1, c->fct_items, c->mx_items, c->derr};
+  RunTable T{c->ddesc + c->cur, 1, c->fct_items, c->mx_items, c->derr, c->fx_items, c->fz_items};
   mark(c, ST_FCT, s);
-  CK(launch_fct_table(T, c->fct_tx, c->fct_grid, s), "fct_fused_kernel");
+  if (c->fct_mode == YMKH_FCT_SPLIT) {
+    CK(launch_fct_split_table(T, c->fx_grid, c->fz_grid, s), "fct_x/fct_z kernels");
+    g_launches++;
+  } else {
+    CK(launch_fct_table(T, c->fct_tx, c->fct_grid, s), "fct_fused_kernel");
+  }
   mark(c, ST_MAXWELL, s);
   CK(launch_maxwell_table(T, c->mx_grid, s), "maxwell_fused_kernel");
   g_launches += 2;
@@ -528,6 +562,13 @@ int ymkh_set_fct_shape(ymkh_ctx* c, int tx, int seg) {
   return upload_desc(c);
 }
 
+int ymkh_set_fct_mode(ymkh_ctx* c, int mode) {
+  if (!c || (mode != YMKH_FCT_FUSED && mode != YMKH_FCT_SPLIT)) return set_err(YMKH_EINVAL, "bad FCT mode");
+  drop_graphs(c);
+  c->fct_mode = mode;
+  return upload_desc(c);
+}
+
 int ymkh_get_fct_shape(ymkh_ctx* c, int* tx, int* seg) {
   if (!c) return set_err(YMKH_EINVAL, "null context");
   if (tx) *tx = c->fct_tx;
@@ -600,6 +641,7 @@ int ymkh_destroy(ymkh_ctx* c) {
   if (c->mcol) cudaFree(c->mcol);
   if (c->derr) cudaFree(c->derr);
   if (c->ddesc) cudaFree(c->ddesc);
+  if (c->xscratch) cudaFree(c->xscratch);
   delete c;
   return 0;
 }
@@ -629,8 +671,9 @@ struct ymkh_batch {
   std::vector<ymkh_ctx*> runs;
   RunDesc* ddesc = nullptr;  // [2][cap]: tables for the members' current / next buffers
   int cap = 0;
-  int fct_items = 0, mx_items = 0;
-  int tb = 64, fct_grid = 0, mx_grid = 0;
+  int fct_items = 0, mx_items = 0, fx_items = 0, fz_items = 0;
+  int tb = 64, fct_grid = 0, mx_grid = 0, fx_grid = 0, fz_grid = 0;
+  int fct_mode = YMKH_FCT_SPLIT;
   unsigned* derr = nullptr;
   bool dirty = true;
   int parity = 0;            // steps taken since the tables were built, mod 2
@@ -654,11 +697,22 @@ int batch_build(ymkh_batch* b) {
     CK(cudaMalloc(&b->ddesc, 2 * (size_t)b->cap * sizeof(RunDesc)), "cudaMalloc batch descriptors");
   }
   std::vector<RunDesc> h(2 * (size_t)std::max(n, 1));
-  int f0 = 0, m0 = 0;
+  int f0 = 0, m0 = 0, x0 = 0, z0 = 0;
   for (int i = 0; i < n; ++i) {
     ymkh_ctx* c = b->runs[i];
+    if (b->fct_mode == YMKH_FCT_SPLIT && !c->xscratch) {
+      const int keep = c->fct_mode;
+      c->fct_mode = YMKH_FCT_SPLIT;
+      int rc = ensure_xscratch(c);
+      c->fct_mode = keep;
+      if (rc) return rc;
+    }
     RunDesc d0 = make_desc(c, c->cur, b->tb, f0, m0);
     RunDesc d1 = make_desc(c, 1 - c->cur, b->tb, f0, m0);
+    d0.fx_item0 = d1.fx_item0 = x0;
+    d0.fz_item0 = d1.fz_item0 = z0;
+    x0 += items_fx(d0, c->nz);
+    z0 += items_fz(d0, c->nz);
     // finer segments than a lone run needs: items of many runs share the GPU
     d0.fct_seg = d1.fct_seg = std::min(c->nz, 128);
     d0.mx_seg = d1.mx_seg = std::min(c->nz, 128);
@@ -671,6 +725,8 @@ int batch_build(ymkh_batch* b) {
   }
   b->fct_items = f0;
   b->mx_items = m0;
+  b->fx_items = x0;
+  b->fz_items = z0;
   if (n) {
     CK(cudaMemcpy(b->ddesc, h.data(), (size_t)n * sizeof(RunDesc), cudaMemcpyHostToDevice), "upload batch table");
     CK(cudaMemcpy(b->ddesc + b->cap, h.data() + n, (size_t)n * sizeof(RunDesc), cudaMemcpyHostToDevice),
@@ -685,8 +741,11 @@ int batch_build(ymkh_batch* b) {
 int batch_step_once(ymkh_batch* b, cudaStream_t s) {
   const int n = (int)b->runs.size();
   if (!n) return 0;
-  RunTable T{b->ddesc + (size_t)b->parity * b->cap, n, b->fct_items, b->mx_items, b->derr};
-  CK(launch_fct_table(T, b->tb, b->fct_grid, s), "fct_fused_kernel (batch)");
+  RunTable T{b->ddesc + (size_t)b->parity * b->cap, n, b->fct_items, b->mx_items, b->derr, b->fx_items, b->fz_items};
+  if (b->fct_mode == YMKH_FCT_SPLIT)
+    CK(launch_fct_split_table(T, b->fx_grid, b->fz_grid, s), "fct_x/fct_z kernels (batch)");
+  else
+    CK(launch_fct_table(T, b->tb, b->fct_grid, s), "fct_fused_kernel (batch)");
   CK(launch_maxwell_table(T, b->mx_grid, s), "maxwell_fused_kernel (batch)");
   g_launches += 2;
   for (ymkh_ctx* c : b->runs) {
@@ -708,6 +767,8 @@ int ymkh_batch_create(ymkh_batch** out) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   b->fct_grid = sms * std::max(1, fct_ctas_per_sm(b->tb));
   b->mx_grid = sms * std::max(1, maxwell_ctas_per_sm());
+  b->fx_grid = sms * std::max(1, fct_split_ctas_per_sm(0)) * 4;
+  b->fz_grid = sms * std::max(1, fct_split_ctas_per_sm(1)) * 4;
   if (cudaMalloc(&b->derr, sizeof(unsigned)) != cudaSuccess || cudaMemset(b->derr, 0, sizeof(unsigned)) != cudaSuccess) {
     delete b;
     return set_err(YMKH_ENOMEM, "cudaMalloc batch error word");
@@ -806,6 +867,13 @@ int ymkh_batch_check(ymkh_batch* b, void* stream) {
     cudaMemsetAsync(b->derr, 0, sizeof(unsigned), (cudaStream_t)stream);
     return set_err(YMKH_ECUDA, "a bounded in-kernel wait timed out (error word %u)", h);
   }
+  return 0;
+}
+
+int ymkh_batch_set_fct_mode(ymkh_batch* b, int mode) {
+  if (!b || (mode != YMKH_FCT_FUSED && mode != YMKH_FCT_SPLIT)) return set_err(YMKH_EINVAL, "bad FCT mode");
+  b->fct_mode = mode;
+  b->dirty = true;
   return 0;
 }
 

@@ -191,9 +191,13 @@ namespace ymkh {
 struct RunDesc {
   State in;
   State out;
+  State xsw;  // x-swept fluid scratch of the split FCT form (fluid arrays only)
   StepParams p;
   int fct_nstrips, fct_seg, fct_item0, fct_bulk;
   int mx_nstrips, mx_seg, mx_item0, mx_bulk;
+  int fx_nstrips, fx_item0;           // split FCT, x pass: items (strip, row, beam)
+  int fz_ncols, fz_seg, fz_item0;     // split FCT, z pass: items (column block, segment)
+  int pad_;
 };
 
 struct RunTable {
@@ -201,7 +205,19 @@ struct RunTable {
   int nruns;
   int fct_items, mx_items;
   unsigned* err;  // device error word of the bounded in-kernel waits
+  int fx_items, fz_items;
 };
+
+// Run owning item g of the split FCT's x pass (which = 0) or z pass (1).
+__device__ __forceinline__ int find_run_split(const RunDesc* runs, int nruns, int g, int which) {
+  int lo = 0, hi = nruns - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    const int i0 = which ? runs[mid].fz_item0 : runs[mid].fx_item0;
+    if (i0 <= g) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
 
 // Index of the run owning flattened item g (binary search on item0).
 __device__ __forceinline__ int find_run(const RunDesc* runs, int nruns, int g, bool maxwell) {
@@ -227,5 +243,9 @@ int fct_nstrips(int nx, int tb);
 int maxwell_nstrips(int nx);
 int fct_bulk_ok(const StepParams& p, int tb);
 int maxwell_bulk_ok(const StepParams& p);
+cudaError_t launch_fct_split_table(const RunTable& T, int grid_x, int grid_z, cudaStream_t s);
+int fct_split_ctas_per_sm(int which);
+int fctx_nstrips(int nx);
+int fctz_ncols(int nx);
 
 }  // namespace ymkh

@@ -224,3 +224,22 @@ def test_10k_step_history_vs_reference(cuda, ref):
     ar, ag = np.array(ar), np.array(ag)
     assert np.all(np.abs(ag - ar) <= 1e-9 * np.abs(ar)), (ar, ag)
     run.close()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fct_forms_identical(cuda, name):
+    """The fused single-pass FCT and the split x/z-pass FCT give the same
+    state bit for bit (they are two schedules of the same arithmetic)."""
+    from kh_simulations_b200 import _lib
+    from kh_simulations_b200.run import KHRun
+
+    cfg = config(name)
+    out = []
+    for mode in (_lib.FCT_FUSED, _lib.FCT_SPLIT):
+        run = KHRun(cfg)
+        _lib.check(run.lib.ymkh_set_fct_mode(run.ctx, mode), "ymkh_set_fct_mode")
+        run.init()
+        run.step(4)
+        out.append(run.state_numpy())
+        run.close()
+    assert np.array_equal(out[0], out[1]), f"max |diff| {np.abs(out[0] - out[1]).max()}"
