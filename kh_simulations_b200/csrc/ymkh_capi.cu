@@ -381,6 +381,7 @@ int ymkh_create(const ymkh_grid* grid, const ymkh_params* params, ymkh_ctx** out
   CK(prepare_fct(64), "FCT kernel attributes");
   CK(prepare_fct(128), "FCT kernel attributes");
   CK(prepare_maxwell(), "Maxwell kernel attributes");
+  CK(prepare_fct_split(), "split FCT kernel attributes");
   choose_launch_shape(c);
   CK(prepare_column(c->nz), "column kernel attributes");
   const int np = energy_nparts(c->N);
@@ -765,6 +766,9 @@ int ymkh_batch_create(ymkh_batch** out) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  for (int tb : {32, 64, 128}) prepare_fct(tb);
+  prepare_maxwell();
+  prepare_fct_split();
   b->fct_grid = sms * std::max(1, fct_ctas_per_sm(b->tb));
   b->mx_grid = sms * std::max(1, maxwell_ctas_per_sm());
   b->fx_grid = sms * std::max(1, fct_split_ctas_per_sm(0)) * 4;

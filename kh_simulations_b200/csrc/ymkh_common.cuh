@@ -245,6 +245,7 @@ int fct_bulk_ok(const StepParams& p, int tb);
 int maxwell_bulk_ok(const StepParams& p);
 cudaError_t launch_fct_split_table(const RunTable& T, int grid_x, int grid_z, cudaStream_t s);
 int fct_split_ctas_per_sm(int which);
+cudaError_t prepare_fct_split();
 int fctx_nstrips(int nx);
 int fctz_ncols(int nx);
 

@@ -165,18 +165,36 @@ __global__ void __launch_bounds__(2 * XT)
 }
 
 // ------------------------------------------------------------------ z pass
-// One thread per (column, beam, half) streams a z-segment.  The pipeline
-// registers are those of the fused kernel (ymkh_fct.cu).
-constexpr int ZB = 32;  // columns per warp-wide group
+// One thread per (column, beam, half) streams a z-segment.  Each lane stages
+// its own inputs for the next ZNST-1 rows in a per-warp shared-memory ring
+// with 8-byte cp.async (no registers held by loads in flight), so every warp
+// keeps ~2 rows of loads in flight while its z-pipeline (the registers of
+// the fused kernel) consumes the current row.
+constexpr int ZB = 32;    // columns per warp
+constexpr int ZNST = 3;   // ring depth (rows)
+constexpr int ZNV = 30;   // staged values per lane per row
+
+// slot layout per lane and row
+enum {
+  ZV_X = 0,          // x-swept values of the half's 3 variables
+  ZV_N = 3, ZV_PZ = 4, ZV_Q = 5,  // n, pz, Q1..Q3 (start of step)
+  ZV_PX = 8,         // half 0: px
+  ZV_BY = 9,         // half 0: By[c] at (x, zr), (xm, zr), (x, zm), (xm, zm): 9 + 4c + j
+  ZV_EZ = 21,        // half 0: Ez[c] at zr, zm: 21 + 2c + j
+  ZV_NZP = 27, ZV_NZM = 28,  // half 0, warm_T: n at zp, zm
+  ZV_AZ = 9          // half 1: Az[c] at zr, zm: 9 + 2c + j
+};
 
 __global__ void __launch_bounds__(128)
     fct_z_kernel(const __grid_constant__ RunTable T) {
   __shared__ RunDesc rd;
+  extern __shared__ __align__(16) double zring[];  // [4 warps][ZNST][ZNV][ZB]
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;  // 4 warps: (beam, half)
   const int beam = warp >> 1;
   const int half = warp & 1;
   const int k0 = 3 * half;
+  double (*rg)[ZNV][ZB] = reinterpret_cast<double (*)[ZNV][ZB]>(zring + (size_t)warp * ZNST * ZNV * ZB);
   int cur_run = -1;
 
   for (int item = blockIdx.x; item < T.fz_items; item += gridDim.x) {
@@ -199,46 +217,89 @@ __global__ void __launch_bounds__(128)
     const int xc = active ? x : nx - 1;  // inactive lanes read a valid cell and emit nothing
     const int xcm = p.periodic_x ? (xc == 0 ? nx - 1 : xc - 1) : (xc == 0 ? 0 : xc - 1);
     const bool wall = !p.periodic_x;
+    const bool warm = p.warm_T > 0.0;
     const double dt = p.dt, dtdz = p.dt / p.dz;
     const State& st = rd.in;
     double* const* fl = beam ? st.b : st.a;
     double* const* xsw = beam ? rd.xsw.b : rd.xsw.a;
     double* const* dst = beam ? rd.out.b : rd.out.a;
 
+    auto issue = [&](int rr, int s) {
+      const int zr = zclamp(rr, nz);
+      const int zm = (zr == 0) ? nz - 1 : zr - 1;
+      const size_t row = (size_t)zr * nx, rowm = (size_t)zm * nx;
+      double (*sl)[ZB] = rg[s];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) cp_async8(&sl[ZV_X + j][lane], xsw[k0 + j] + row + xc);
+      cp_async8(&sl[ZV_N][lane], fl[FN] + row + xc);
+      cp_async8(&sl[ZV_PZ][lane], fl[FPZ] + row + xc);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) cp_async8(&sl[ZV_Q + c][lane], fl[FQ1 + c] + row + xc);
+      if (half == 0) {
+        cp_async8(&sl[ZV_PX][lane], fl[FPX] + row + xc);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const double* By = st.f[BY1 + c];
+          cp_async8(&sl[ZV_BY + 4 * c + 0][lane], By + row + xc);
+          cp_async8(&sl[ZV_BY + 4 * c + 1][lane], By + row + xcm);
+          cp_async8(&sl[ZV_BY + 4 * c + 2][lane], By + rowm + xc);
+          cp_async8(&sl[ZV_BY + 4 * c + 3][lane], By + rowm + xcm);
+          cp_async8(&sl[ZV_EZ + 2 * c + 0][lane], st.f[EZ1 + c] + row + xc);
+          cp_async8(&sl[ZV_EZ + 2 * c + 1][lane], st.f[EZ1 + c] + rowm + xc);
+        }
+        if (warm) {
+          const int zp = (zr == nz - 1) ? 0 : zr + 1;
+          cp_async8(&sl[ZV_NZP][lane], fl[FN] + (size_t)zp * nx + xc);
+          cp_async8(&sl[ZV_NZM][lane], fl[FN] + rowm + xc);
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          cp_async8(&sl[ZV_AZ + 2 * c + 0][lane], st.f[AZ1 + c] + row + xc);
+          cp_async8(&sl[ZV_AZ + 2 * c + 1][lane], st.f[AZ1 + c] + rowm + xc);
+        }
+      }
+    };
+
+    const int r_first = zs - 3, r_last = ze + 2;
+#pragma unroll
+    for (int k = 0; k < ZNST - 1; ++k) {
+      if (r_first + k <= r_last) issue(r_first + k, k);
+      cp_async_commit();
+    }
+
     double V1[3], f1[3], d1[3], L2[3], N4[3], N3[3], N2[3], A2[3], F3[3], S1[3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) V1[j] = f1[j] = d1[j] = L2[j] = N4[j] = N3[j] = N2[j] = A2[j] = F3[j] = S1[j] = 0.0;
     double U1 = 0.0, mu1 = 0.0;
 
-    for (int rr = zs - 3; rr <= ze + 2; ++rr) {
-      const int zr = zclamp(rr, nz);
-      const int zm = (zr == 0) ? nz - 1 : zr - 1;
-      const size_t row = (size_t)zr * nx, rowm = (size_t)zm * nx;
+    for (int rr = r_first, it = 0; rr <= r_last; ++rr, ++it) {
+      cp_async_wait<ZNST - 2>();
+      __syncwarp();
+      const double (*sl)[ZB] = rg[it % ZNST];
       double Vx[3];
 #pragma unroll
-      for (int j = 0; j < 3; ++j) Vx[j] = xsw[k0 + j][row + xc];
-      const double n0 = fmax(fl[FN][row + xc], 0.05);
-      const double vz = fl[FPZ][row + xc] / n0;
-      const double q1 = fl[FQ1][row + xc], q2 = fl[FQ2][row + xc], q3 = fl[FQ3][row + xc];
+      for (int j = 0; j < 3; ++j) Vx[j] = sl[ZV_X + j][lane];
+      const double n0 = fmax(sl[ZV_N][lane], 0.05);
+      const double vz = sl[ZV_PZ][lane] / n0;
+      const double q1 = sl[ZV_Q + 0][lane], q2 = sl[ZV_Q + 1][lane], q3 = sl[ZV_Q + 2][lane];
       double S[3];
       if (half == 0) {
         // YM_Fluid.cu:44, 52-67 (src.pz) and :76-79 (warm closure)
-        const double vx = fl[FPX][row + xc] / n0;
+        const double vx = sl[ZV_PX][lane] / n0;
         double acc = 0.0;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          const double* By = st.f[BY1 + c];
-          const double* Ez = st.f[EZ1 + c];
-          const double by = 0.25 * (By[row + xc] + By[row + xcm] + By[rowm + xc] + By[rowm + xcm]);
-          const double ez = 0.5 * (Ez[row + xc] + Ez[rowm + xc]);
+          const double by = 0.25 * (sl[ZV_BY + 4 * c + 0][lane] + sl[ZV_BY + 4 * c + 1][lane] +
+                                    sl[ZV_BY + 4 * c + 2][lane] + sl[ZV_BY + 4 * c + 3][lane]);
+          const double ez = 0.5 * (sl[ZV_EZ + 2 * c + 0][lane] + sl[ZV_EZ + 2 * c + 1][lane]);
           const double qa = (c == 0) ? q1 : (c == 1) ? q2 : q3;
           const double term = qa * (ez - vx * by);
           acc = (c == 0) ? term : acc + term;
         }
         double sz = -acc;
-        if (p.warm_T > 0.0) {
-          const int zp = (zr == nz - 1) ? 0 : zr + 1;
-          const double dndz = (fl[FN][(size_t)zp * nx + xc] - fl[FN][rowm + xc]) / (2.0 * p.dz);
+        if (warm) {
+          const double dndz = (sl[ZV_NZP][lane] - sl[ZV_NZM][lane]) / (2.0 * p.dz);
           sz -= p.warm_T * dndz;
         }
         S[0] = 0.0;
@@ -248,10 +309,17 @@ __global__ void __launch_bounds__(128)
         // YM_Fluid.cu:99-107 (colour precession)
         double azn[3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) azn[c] = 0.5 * (st.f[AZ1 + c][row + xc] + st.f[AZ1 + c][rowm + xc]);
+        for (int c = 0; c < 3; ++c) azn[c] = 0.5 * (sl[ZV_AZ + 2 * c + 0][lane] + sl[ZV_AZ + 2 * c + 1][lane]);
         S[0] = p.alpha * vz * (q2 * azn[2] - q3 * azn[1]);
         S[1] = p.alpha * vz * (q3 * azn[0] - q1 * azn[2]);
         S[2] = p.alpha * vz * (q1 * azn[1] - q2 * azn[0]);
+      }
+      __syncwarp();
+      // refill the slot consumed last iteration (row rr + ZNST - 1)
+      {
+        const int rn = rr + ZNST - 1;
+        if (rn <= r_last) issue(rn, (it + ZNST - 1) % ZNST);
+        cp_async_commit();
       }
       const double e = fct_eps(U1, vz, dtdz);
       double nu, mu;
@@ -292,16 +360,24 @@ __global__ void __launch_bounds__(128)
         for (int j = 0; j < 3; ++j) dst[k0 + j][gi] = outv[j];
       }
     }
+    cp_async_wait<0>();
+    __syncwarp();
   }
 }
 
 int fctz_ncols(int nx) { return (nx + ZB - 1) / ZB; }
 
+constexpr size_t fctz_smem_bytes() { return (size_t)4 * ZNST * ZNV * ZB * sizeof(double); }
+
+cudaError_t prepare_fct_split() {
+  return cudaFuncSetAttribute(fct_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fctz_smem_bytes());
+}
+
 cudaError_t launch_fct_split_table(const RunTable& T, int grid_x, int grid_z, cudaStream_t s) {
   fct_x_kernel<<<std::max(1, std::min(T.fx_items, grid_x)), 2 * XT, 0, s>>>(T);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  fct_z_kernel<<<std::max(1, std::min(T.fz_items, grid_z)), 128, 0, s>>>(T);
+  fct_z_kernel<<<std::max(1, std::min(T.fz_items, grid_z)), 128, fctz_smem_bytes(), s>>>(T);
   return cudaGetLastError();
 }
 
@@ -310,7 +386,7 @@ int fct_split_ctas_per_sm(int which) {
   if (which == 0)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fct_x_kernel, 2 * XT, 0);
   else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fct_z_kernel, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fct_z_kernel, 128, fctz_smem_bytes());
   return n;
 }
 
