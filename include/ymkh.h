@@ -150,7 +150,7 @@ int ymkh_set_current_buffer(ymkh_ctx* ctx, int which);
 int ymkh_set_graph_steps(ymkh_ctx* ctx, int nsteps_per_graph);
 int ymkh_set_fct_shape(ymkh_ctx* ctx, int strip_width, int segment_rows);
 int ymkh_get_fct_shape(ymkh_ctx* ctx, int* strip_width, int* segment_rows);
-int ymkh_set_fct_mode(ymkh_ctx* ctx, int mode);  /* YMKH_FCT_*; chosen per size class by the autotuner */
+int ymkh_set_fct_mode(ymkh_ctx* ctx, int mode);  /* YMKH_FCT_* (default FUSED); the autotuner picks per size class */
 
 /* Device time per stage over nsteps uncaptured steps (CUDA events between
  * stages on `stream`), accumulated in out_ms[0..6]: FCT, Maxwell,

@@ -4,7 +4,8 @@ For a grid-size class (NZ and NX rounded to powers of two, band filter on or
 off) it times the fused FCT kernel for each candidate strip width (the tile
 shape: 32, 64 or 128 x-sweep positions per beam) and z-segment length
 (rows per work item, which sets how often the 3-row z halo is re-swept),
-then the number of steps per captured CUDA graph, and keeps the fastest.
+then the split FCT form, then the number of steps per captured CUDA graph,
+and keeps the fastest.
 Results are cached in a JSON table (``tuned.json`` beside this module, or
 the path in ``KH_TUNING_FILE``) that ``KHRun(tune=True)`` consults.
 
@@ -55,16 +56,28 @@ def tune(run, reps: int = 3, graph_candidates=(2, 4, 8), save: bool = True) -> d
     out = (C.c_float * 8)()
     best = None
     timings = {}
-    for tb, seg in candidates(run.d.nx, run.d.nz):
-        _lib.check(lib.ymkh_set_fct_shape(run.ctx, tb, seg), "ymkh_set_fct_shape")
+    def fct_ms():
         _lib.check(lib.ymkh_stage_times(run.ctx, 1, C.c_void_p(stream.cuda_stream), out, 8), "warm-up")
         _lib.check(lib.ymkh_stage_times(run.ctx, reps, C.c_void_p(stream.cuda_stream), out, 8), "stage times")
-        ms = out[0] / reps
+        return out[0] / reps
+
+    _lib.check(lib.ymkh_set_fct_mode(run.ctx, _lib.FCT_FUSED), "ymkh_set_fct_mode")
+    for tb, seg in candidates(run.d.nx, run.d.nz):
+        _lib.check(lib.ymkh_set_fct_shape(run.ctx, tb, seg), "ymkh_set_fct_shape")
+        ms = fct_ms()
         timings[f"{tb}x{seg}"] = ms
         if best is None or ms < best[0]:
-            best = (ms, tb, seg)
-    _, tb, seg = best
+            best = (ms, _lib.FCT_FUSED, tb, seg)
+    _, _, tb, seg = best
     _lib.check(lib.ymkh_set_fct_shape(run.ctx, tb, seg), "ymkh_set_fct_shape")
+    # the split form (x pass + z-streaming pass through a scratch copy)
+    _lib.check(lib.ymkh_set_fct_mode(run.ctx, _lib.FCT_SPLIT), "ymkh_set_fct_mode")
+    ms = fct_ms()
+    timings["split"] = ms
+    if ms < best[0]:
+        best = (ms, _lib.FCT_SPLIT, tb, seg)
+    mode = best[1]
+    _lib.check(lib.ymkh_set_fct_mode(run.ctx, mode), "ymkh_set_fct_mode")
     gbest = None
     for g in graph_candidates:
         _lib.check(lib.ymkh_set_graph_steps(run.ctx, g), "ymkh_set_graph_steps")
@@ -80,7 +93,8 @@ def tune(run, reps: int = 3, graph_candidates=(2, 4, 8), save: bool = True) -> d
         if gbest is None or ms < gbest[0]:
             gbest = (ms, g)
     _lib.check(lib.ymkh_set_graph_steps(run.ctx, gbest[1]), "ymkh_set_graph_steps")
-    entry = {"fct_strip": tb, "fct_segment": seg, "graph_steps": gbest[1], "fct_ms": best[0],
+    entry = {"fct_mode": "split" if mode == _lib.FCT_SPLIT else "fused", "fct_strip": tb, "fct_segment": seg,
+             "graph_steps": gbest[1], "fct_ms": best[0],
              "step_ms": gbest[0], "fct_candidates_ms": timings}
     if save:
         table = load_table()
@@ -96,5 +110,7 @@ def apply(run) -> bool:
         return False
     lib = _lib.load()
     _lib.check(lib.ymkh_set_fct_shape(run.ctx, int(e["fct_strip"]), int(e["fct_segment"])), "ymkh_set_fct_shape")
+    mode = _lib.FCT_SPLIT if e.get("fct_mode") == "split" else _lib.FCT_FUSED
+    _lib.check(lib.ymkh_set_fct_mode(run.ctx, mode), "ymkh_set_fct_mode")
     _lib.check(lib.ymkh_set_graph_steps(run.ctx, int(e["graph_steps"])), "ymkh_set_graph_steps")
     return True
