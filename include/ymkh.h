@@ -215,6 +215,23 @@ int ymkh_batch_destroy(ymkh_batch* batch);
  * points, all threads).  Used to report launch counts. */
 long long ymkh_launch_count(void);
 
+/* Total energy of a caller-bound state without any device allocation by the
+ * library (no context; no reference counterpart: the reference sums energy
+ * through a buffer it allocates, ymgpu2d/YM_Energy.cu:23-32).  For callers
+ * that cannot allow cudaMalloc: an arena that owns the device memory, a
+ * multi-stream loop that must not be synchronised by allocation, or code
+ * holding only the 24 state arrays.  Same kernels and summation order as
+ * ymkh_energy_async, so the same total bit for bit.  state: 24 device
+ * pointers in state order; writes one double to dev_out on `stream`.
+ * Partial sums live in a static device array sized for at most
+ * YMKH_NOALLOC_MAX_CELLS cells; larger grids return YMKH_EINVAL.  The first
+ * call on each device (that device current) looks up the array's address
+ * (cudaGetSymbolAddress) and caches it: make it before any stream capture.
+ * Calls that overlap on one device share the array and race: keep them on
+ * one stream or one after another. */
+#define YMKH_NOALLOC_MAX_CELLS 134217728
+int ymkh_energy_noalloc(double* const* state, int nx, int nz, double* dev_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

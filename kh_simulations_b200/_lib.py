@@ -13,6 +13,7 @@ LIB_PATH = _PKG / "libymkh.so"
 
 NFIELDS, NFLUID, NSTATE = 12, 6, 24
 MAX_EXTRA_BANDS = 4
+NOALLOC_MAX_CELLS = 134217728  # YMKH_NOALLOC_MAX_CELLS
 FILTER_DFT = 0
 FCT_FUSED, FCT_SPLIT = 0, 1
 
@@ -95,6 +96,7 @@ _SIGS = {
     "ymkh_batch_destroy": (C.c_int, [C.c_void_p]),
     "ymkh_twiddles": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "ymkh_launch_count": (C.c_longlong, []),
+    "ymkh_energy_noalloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "ymkh_stage_times": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_float), C.c_int]),
 }
 

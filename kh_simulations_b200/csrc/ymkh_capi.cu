@@ -898,3 +898,10 @@ int ymkh_batch_destroy(ymkh_batch* b) {
 }
 
 }  // extern "C"
+
+namespace ymkh {
+// Error reporting and launch counting for entry points defined in other
+// translation units (ymkh_noalloc.cu).
+int capi_error(int code, const char* msg) { return set_err(code, "%s", msg); }
+void capi_count_launches(int n) { g_launches += n; }
+}  // namespace ymkh

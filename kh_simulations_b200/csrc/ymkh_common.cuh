@@ -131,6 +131,8 @@ int energy_nparts(size_t N);
 cudaError_t launch_mode_amp(const double* az2, const double* az3, int nx, int nz, int k, double* colbuf, double* out,
                             cudaStream_t s);
 cudaError_t launch_init(const State& st, const InitArgs& a, cudaStream_t s);
+int capi_error(int code, const char* msg);
+void capi_count_launches(int n);
 
 }  // namespace ymkh
 
