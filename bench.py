@@ -156,10 +156,11 @@ def max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
-def cpu_oracle_rate(workload: str, steps: int, threads: int | None = None) -> dict:
+def cpu_oracle_rate(workload: str, steps: int, threads: int | None = None, min_seconds: float = 0.0) -> dict:
     """The FP64 OpenMP oracle on a bounded sample of the workload: the full
     shear extent and NZ reduced to 256 rows (the step's per-cell work does not
-    depend on NZ when no band filter runs)."""
+    depend on NZ when no band filter runs).  Runs `steps` steps, then more
+    one at a time until `min_seconds` of work have been timed."""
     import numpy as np
 
     from kh_simulations_b200._lib import Grid
@@ -186,6 +187,10 @@ def cpu_oracle_rate(workload: str, steps: int, threads: int | None = None) -> di
     t0 = time.perf_counter()
     orc.step(g, p, st, steps)
     dt = time.perf_counter() - t0
+    while dt < min_seconds:
+        orc.step(g, p, st, 1)
+        steps += 1
+        dt = time.perf_counter() - t0
     return {"value": nx * nz * steps / dt, "unit": "cell-steps/s", "cores": orc.threads(), "kind": "port",
             "sample": f"FP64 OpenMP oracle, {steps} step(s) of the same physics on {nz}x{nx} (NZ x NX) = "
                       f"{nx * nz} cells, no band filter, {dt:.2f} s"}
@@ -343,7 +348,7 @@ def main() -> int:
     if args.with_filter_line and args.filter == "ref" and d.nz > 1024:
         line["filter_keep"] = filter_keep_rate(args, dev)
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_oracle_rate(args.workload, 1)
+        line["cpu_baseline"] = cpu_oracle_rate(args.workload, 1, min_seconds=10.0)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
