@@ -121,41 +121,6 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup():
-    import torch
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device(f"cuda:{local}"))
-    return world, rank, local
-
-
-def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.barrier()
-
-
-def max_over_ranks(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
 def cpu_oracle_rate(workload: str, steps: int, threads: int | None = None, min_seconds: float = 0.0) -> dict:
     """The FP64 OpenMP oracle on a bounded sample of the workload: the full
     shear extent and NZ reduced to 256 rows (the step's per-cell work does not
@@ -265,9 +230,16 @@ def main() -> int:
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
-    world, rank, local = dist_setup()
+    from kh_simulations_b200 import replicas
+
     if args.impl == "reference":
-        return run_reference(args, world, rank, local)
+        # rank 0 alone times the reference on the host cores; other ranks
+        # exit at once (no process group: the arm has no collective)
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        return run_reference(args, world, rank, int(os.environ.get("LOCAL_RANK", "0")))
+    rk = replicas.init("nccl")
+    world, rank, local = rk.world, rk.rank, rk.local
 
     import torch
 
@@ -285,7 +257,7 @@ def main() -> int:
     stream = torch.cuda.Stream(device=dev)
     run.step(args.warmup, stream)
     torch.cuda.synchronize(dev)
-    barrier(world)
+    replicas.barrier(rk)
 
     sampler = ClockSampler(dev.index if dev.index is not None else 0)
     sampler.start()
@@ -301,9 +273,9 @@ def main() -> int:
     launches = _lib.launch_count() - l0
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
-    ms_max = max_over_ranks(ms, world)
-    barrier(world)
-    value = cells * args.steps * world / (ms_max / 1e3)
+    ms_max = replicas.max_over_ranks(ms, rk)
+    replicas.barrier(rk)
+    value = replicas.aggregate_rate(cells * args.steps, ms_max, rk)
 
     # per-stage device times (separate uncaptured pass, events between stages)
     nst = 3
@@ -340,7 +312,7 @@ def main() -> int:
             "stage_ms": stage_ms, "clocks": clocks, "gpu_launches": launches}
 
     if not args.no_e2e:
-        line["e2e"] = e2e_rate(run, args, stream, world)
+        line["e2e"] = e2e_rate(run, args, stream, rk)
     run.close()
     del run
     torch.cuda.empty_cache()
@@ -351,24 +323,27 @@ def main() -> int:
         line["cpu_baseline"] = cpu_oracle_rate(args.workload, 1, min_seconds=10.0)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.destroy_process_group()
+    replicas.finish(rk)
     return 0
 
 
-def e2e_rate(run, args, stream, world) -> dict:
+def e2e_rate(run, args, stream, rk) -> dict:
     """Same metric through the public API with host buffers: upload the
     state from pinned host memory, K steps each followed by the energy
-    read back (the reference's per-step diagnostic), download the state."""
+    read back (the reference's per-step diagnostic), download the state.
+    Timed with CUDA events on the stream around all of it (host waits
+    included), max over ranks."""
     import torch
+
+    from kh_simulations_b200 import replicas
 
     st_host = run.state.to("cpu").pin_memory()
     out_host = torch.empty_like(st_host).pin_memory()
     torch.cuda.synchronize()
-    barrier(world)
-    t0 = time.perf_counter()
+    replicas.barrier(rk)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
     with torch.cuda.stream(stream):
         run.buf[0].copy_(st_host, non_blocking=True)
     run.lib.ymkh_set_current_buffer(run.ctx, 0)
@@ -377,12 +352,12 @@ def e2e_rate(run, args, stream, world) -> dict:
         run.energy(stream)
     with torch.cuda.stream(stream):
         out_host.copy_(run.state, non_blocking=True)
-    stream.synchronize()
-    dt = time.perf_counter() - t0
-    dt = max_over_ranks(dt, world)
+    e1.record(stream)
+    e1.synchronize()
+    ms = replicas.max_over_ranks(e0.elapsed_time(e1), rk)
     cells = run.d.nx * run.d.nz
     sb = st_host.numel() * 8
-    return {"value": cells * args.steps * world / dt, "unit": "cell-steps/s",
+    return {"value": replicas.aggregate_rate(cells * args.steps, ms, rk), "unit": "cell-steps/s",
             "h2d_bytes_per_step": sb / args.steps, "d2h_bytes_per_step": 8 + sb / args.steps,
             "note": "state uploaded once and downloaded once per K-step call; energy read back every step"}
 
