@@ -227,6 +227,8 @@ def main() -> int:
     ap.add_argument("--with-filter-line", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--batched-runs", type=int, default=64, help="runs in the batched-vs-plain leg (0: skip)")
+    ap.add_argument("--served-seconds", type=float, default=3.0, help="arrival window of the served leg (0: skip)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -319,6 +321,10 @@ def main() -> int:
 
     if args.with_filter_line and args.filter == "ref" and d.nz > 1024:
         line["filter_keep"] = filter_keep_rate(args, dev)
+    if world == 1 and args.batched_runs > 0:
+        line["batched"] = batched_rate(args, dev, args.batched_runs)
+    if world == 1 and args.served_seconds > 0:
+        line["served"] = served_rate(args, dev, args.served_seconds)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_oracle_rate(args.workload, 1, min_seconds=10.0)
     if rank == 0:
@@ -360,6 +366,107 @@ def e2e_rate(run, args, stream, rk) -> dict:
     return {"value": replicas.aggregate_rate(cells * args.steps, ms, rk), "unit": "cell-steps/s",
             "h2d_bytes_per_step": sb / args.steps, "d2h_bytes_per_step": 8 + sb / args.steps,
             "note": "state uploaded once and downloaded once per K-step call; energy read back every step"}
+
+
+SWEEP_BASE = "alpha_YM = 1.0\nrun_mode = 6\nlx_override = 20\n"
+
+
+def _rel_l2_max(a, b) -> float:
+    """Largest per-array relative L2 difference between two [24, NZ, NX] states."""
+    d = (a - b).reshape(a.shape[0], -1).norm(dim=1)
+    n = b.reshape(b.shape[0], -1).norm(dim=1).clamp_min(1e-300)
+    return float((d / n).max())
+
+
+def batched_rate(args, dev, nruns: int) -> dict:
+    """Uneven sweep of `nruns` runs (seed 1; NZ 128..1024, NX 256..2048):
+    aggregate cell-steps/s of the batched form (one FCT and one Maxwell
+    launch per step over every run's tiles, CUDA graphs) against the same
+    runs stepped one after another through the plain single-run step, from
+    the same state; the two final states are compared run by run."""
+    import torch
+
+    from kh_simulations_b200.batch import KHBatch
+    from kh_simulations_b200.run import KHRun
+    from kh_simulations_b200.server import uneven_sweep
+
+    stream = torch.cuda.Stream(device=dev)
+    runs = [KHRun(c, device=dev) for c in uneven_sweep(1, nruns, SWEEP_BASE)]
+    for r in runs:
+        r.init(stream=stream)
+        r.step(4, stream)  # warm-up: graphs captured, current buffer back to 0
+    torch.cuda.synchronize(dev)
+    s0 = [r.state.clone() for r in runs]
+    cells = sum(r.d.nx * r.d.nz for r in runs)
+    k = max(2, args.steps - args.steps % 2)
+
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for r in runs:
+        r.step(k, stream)
+    e1.record(stream)
+    e1.synchronize()
+    ms_plain = e0.elapsed_time(e1)
+    plain_state = [r.state.clone() for r in runs]
+
+    for r, s in zip(runs, s0):
+        r.set_state(s)
+    torch.cuda.synchronize(dev)
+    batch = KHBatch(device=dev)
+    for r in runs:
+        batch.add(r)
+    batch.step(4, stream)  # warm-up (graph capture); even, so every run is back on buffer 0
+    torch.cuda.synchronize(dev)
+    for r, s in zip(runs, s0):
+        r.set_state(s)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    batch.step(k, stream)
+    e1.record(stream)
+    e1.synchronize()
+    ms_batch = e0.elapsed_time(e1)
+    dev_max = max(_rel_l2_max(r.state, p) for r, p in zip(runs, plain_state))
+    batch.close()
+    for r in runs:
+        r.close()
+    del runs, s0, plain_state
+    torch.cuda.empty_cache()
+    plain = cells * k / (ms_plain / 1e3)
+    batched = cells * k / (ms_batch / 1e3)
+    return {"workload": f"uneven sweep, {nruns} runs (seed 1), {cells} cells, {k} steps",
+            "batched_cell_steps_per_s": batched, "plain_cell_steps_per_s": plain, "batched_over_plain": batched / plain,
+            "max_rel_l2_batched_vs_plain": dev_max, "unit": "cell-steps/s", "timing": "CUDA events, one stream"}
+
+
+def served_rate(args, dev, seconds: float) -> dict:
+    """Served request mix scaled to the bench's time budget: Poisson arrivals
+    at 20 runs/s for `seconds` s (seed 3), cells log-uniform in
+    [128*256, 2048*4096], steps uniform in [20, 200] (the full mix has
+    2000..20000: scaled by 1/100 so both passes finish in seconds), 150 GB
+    admission budget.  Continuous batching (KHServer.serve) against the same
+    requests one by one through the plain step (serve_sequential); p50/p99
+    run latency from arrival to completion; per-request final energies of
+    the two passes are compared."""
+    import math
+
+    from kh_simulations_b200.server import KHServer, poisson_mix
+
+    def mix():
+        return poisson_mix(3, 20.0, seconds, 128 * 256, 2048 * 4096, 20, 200, SWEEP_BASE)
+
+    srv = KHServer(150 << 30, device=dev, chunk=50)
+    served = srv.serve(mix())
+    seq = srv.serve_sequential(mix())
+    ea = {r.rid: r.energy for r in served.requests}
+    de = max((abs(r.energy - ea[r.rid]) / abs(r.energy) for r in seq.requests
+              if math.isfinite(r.energy) and r.energy != 0), default=0.0)
+    a, b = served.summary(), seq.summary()
+    keys = ("requests", "completed", "halted", "makespan_s", "cell_steps_per_s", "p50_latency_s", "p99_latency_s")
+    return {"workload": f"Poisson 20/s for {seconds:g} s (seed 3), 128x256..2048x4096 cells, 20..200 steps, 150 GB budget",
+            "served": {k: a[k] for k in keys}, "sequential": {k: b[k] for k in keys},
+            "served_over_sequential": a["cell_steps_per_s"] / b["cell_steps_per_s"] if b["cell_steps_per_s"] else None,
+            "max_rel_energy_diff": de, "unit": "cell-steps/s", "latency_clock": "host wall clock (arrival to completion)"}
 
 
 def filter_keep_rate(args, dev) -> dict:

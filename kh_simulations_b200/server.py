@@ -283,3 +283,35 @@ def poisson_mix(seed: int, rate: float, duration: float, min_cells: int, max_cel
         out.append(KHRequest(rid, loads(ini, f"req{rid}"), steps, t))
         rid += 1
     return out
+
+
+def cfl_courant(nx: int, nz: int, lx: float = 20.0, lz: float = 2 * math.pi, target: float = 0.4) -> float:
+    """Courant number C (dt = C dx) with dt * sqrt(dx^-2 + dz^-2) <= target,
+    capped at `target`."""
+    dx, dz = lx / nx, lz / nz
+    return min(target, target / (dx * math.sqrt(dx ** -2 + dz ** -2)))
+
+
+def uneven_sweep(seed: int, n: int, base_ini: str = "") -> list:
+    """Seeded uneven-size sweep of n runs: NZ in {128, 256, 512, 1024} and
+    NX in {256, 512, 1024, 2048} drawn uniformly, V0 ~ U[0.02, 0.2], shear
+    width ~ U[0.5, 2], kz in {0..3}, perturbation ~ U[0.05, 0.2], kz = 0
+    suppressed in the runs of even index, CFL-safe Courant number.
+    Returns RunConfigs."""
+    from .config import loads
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        nz = int(rng.choice([128, 256, 512, 1024]))
+        nx = int(rng.choice([256, 512, 1024, 2048]))
+        v0 = rng.uniform(0.02, 0.2)
+        eps = rng.uniform(0.5, 2.0)
+        kz = int(rng.integers(0, 4))
+        amp = rng.uniform(0.05, 0.2)
+        ini = (base_ini + f"k_mode = {kz}\nV0 = {v0:.6f}\neps_override = {eps:.6f}\nperturb_amp = {amp:.6f}\n"
+               f"nz_override = {nz}\nnx_override = {nx}\ncourant_override = {cfl_courant(nx, nz):.6f}\n"
+               f"suppress_kz0 = {1 if i % 2 == 0 else 0}\n")
+        out.append(loads(ini, f"sweep{i}"))
+    return out
+
