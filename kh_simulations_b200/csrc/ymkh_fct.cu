@@ -52,8 +52,10 @@ constexpr int ST_SIZE = 37;
 
 // Per-beam work arrays (units of W), by stage position / interface index
 // (interface j+1/2 stored at j).  Fluxes F, D are dead after phase B, so the
-// limited fluxes reuse their space.
-constexpr int WB_F = 1, WB_D = 7, WB_FLIM = 1, WB_LOR = 13, WB_LNR = 19, WB_SIZE = 25;
+// limited fluxes reuse their space.  WB_SZ holds the pz z-source of the last
+// two rows (slot r & 1): the Q group forms it, the n/px/pz group uses it one
+// row later, which keeps the two groups' work per row about equal.
+constexpr int WB_F = 1, WB_D = 7, WB_FLIM = 1, WB_LOR = 13, WB_LNR = 19, WB_SZ = 25, WB_SIZE = 27;
 
 // Named barrier of one (beam, half) thread group (ids 1..4; 0 is __syncthreads).
 __device__ __forceinline__ void beam_bar(int group, int nthreads) {
@@ -142,6 +144,8 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
 
     if (!bulk)
       for (int i = tid; i < W; i += NT) xtab[i] = xmap(x0 - 4 + i, nx, p.periodic_x);
+    // the pz source before the first row is zero, as the pipeline's start
+    for (int i = tid; i < 2 * 2 * W; i += NT) wk[(size_t)(i / (2 * W)) * WB_SIZE * W + WB_SZ * W + i % (2 * W)] = 0.0;
     __syncthreads();
 
     auto issue_row = [&](int r) {
@@ -353,7 +357,13 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
         const double vz = vz_own;
         const double q1 = fl[FQ1 * W + sp], q2 = fl[FQ2 * W + sp], q3 = fl[FQ3 * W + sp];
         if (half == 0) {
-          // YM_Fluid.cu:67 (src.pz) and :76-79 (warm closure)
+          // the pz source of row r-1, formed by the Q group last row
+          S[0] = 0.0;
+          S[1] = 0.0;
+          S[2] = 0.0;
+          zp.S1[2] = wb[(WB_SZ + ((r - 1) & 1)) * W + sp];
+        } else {
+          // YM_Fluid.cu:67 (src.pz) and :76-79 (warm closure), for the other group
           const double vx = ux_own;
           double by[3], ezn[3];
 #pragma unroll
@@ -367,10 +377,7 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
             const double dndz = (sb[(ST_NZP + beam) * W + sp] - sb[(ST_NZM + beam) * W + sp]) / (2.0 * p.dz);
             sz -= p.warm_T * dndz;
           }
-          S[0] = 0.0;
-          S[1] = 0.0;
-          S[2] = sz;
-        } else {
+          wb[(WB_SZ + (r & 1)) * W + sp] = sz;
           // YM_Fluid.cu:99-107 (colour precession)
           double azn[3];
 #pragma unroll

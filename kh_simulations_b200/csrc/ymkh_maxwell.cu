@@ -25,10 +25,15 @@ namespace ymkh {
 
 namespace {
 
-constexpr int MX_TX = 64;        // output columns per strip
-constexpr int MX_NT = 2 * MX_TX; // threads per CTA
-constexpr int MX_NST = 4;        // stage ring depth (rows q-1, q in use)
-constexpr int MX_W = MX_TX + 4;  // stage row: position s <-> x = x0 - 2 + s
+// 62 output columns per strip: with 128 threads every phase is at most one
+// item per thread (63 velocity columns per beam = 126 items, 62 Ex columns
+// beside 63 Ez columns, Faraday's stores split over both halves), and the
+// strip origin stays even, so staged rows start on 16-byte boundaries.
+constexpr int MX_TX = 62;        // output columns per strip
+constexpr int MX_NV = MX_TX + 1; // velocity / Ez columns (one right neighbour)
+constexpr int MX_NT = 128;       // threads per CTA: [0,64) Ex / By half, [64,128) Ez / store half
+constexpr int MX_NST = 3;        // stage ring depth: rows q-1, q in use, q+1 in flight
+constexpr int MX_W = MX_TX + 4;  // stage row: position s <-> x = x0 - 2 + s (66: even)
 
 // stage offsets in rows of MX_W doubles (every array staged over the full row)
 constexpr int MS_FL = 0;   // 12 fluid arrays
@@ -51,9 +56,11 @@ constexpr size_t maxwell_smem_bytes() {
          (size_t)8 * MX_NST + 16;
 }
 
-__global__ void __launch_bounds__(MX_NT, 3)
+__global__ void __launch_bounds__(MX_NT, 4)
     maxwell_fused_kernel(const __grid_constant__ RunTable T) {
-  constexpr int TX = MX_TX, W = MX_W, NST = MX_NST, NT = MX_NT;
+  constexpr int TX = MX_TX, NV = MX_NV, W = MX_W, NST = MX_NST, NT = MX_NT;
+  static_assert(2 * NV <= NT && TX <= NT / 2 && NV <= NT / 2, "one item per thread per phase");
+  static_assert(W % 2 == 0 && TX % 2 == 0, "even strip origin and row length for 16-byte row copies");
   extern __shared__ __align__(16) double smem[];
   double* const stage = smem;
   double* const wk = smem + (size_t)NST * MS_SIZE * W;
@@ -181,8 +188,8 @@ __global__ void __launch_bounds__(MX_NT, 3)
       const int rq = q & 1, rp = (q - 1) & 1;
 
       // ---- 1: per-cell velocities of row q at x in [x0, x0+TX] (YM_Physics.cu:22-25, 38-41)
-      for (int i = tid; i < 2 * (TX + 1); i += NT) {
-        const int b = i / (TX + 1), k = 2 + (i - b * (TX + 1));
+      if (tid < 2 * NV) {
+        const int b = tid / NV, k = 2 + (tid - b * NV);
         const double* fl = sb + (size_t)(MS_FL + 6 * b) * W;
         const double n = fmax(fl[FN * W + k], 1e-10);
         wk[(MW_V + rq * 4 + b * 2 + 0) * W + k] = fl[FPX * W + k] / n;
@@ -215,7 +222,8 @@ __global__ void __launch_bounds__(MX_NT, 3)
         }
       } else {
         // ---- 2b: Ampère for Ez on row q-1, columns [x0, x0+TX]
-        for (int i = tid - TX; i < TX + 1; i += NT - TX) {
+        const int i = tid - NT / 2;
+        if (i >= 0 && i < NV) {
           const int k = 2 + i;
           double nqz[2][3], vzt[2];
 #pragma unroll
@@ -250,31 +258,42 @@ __global__ void __launch_bounds__(MX_NT, 3)
         __syncthreads();
       }
 
-      // ---- 3: potential and Faraday on row q-1
+      // ---- 3: potential and Faraday on row q-1.  Threads [0, TX) form and
+      // store By and Az of column x0+tid; threads [64, 64+TX) store the new
+      // Ex and Ez of column x0+tid-64.
       const int o = q - 1;
-      if (tid < TX && o >= zs && o < ze && x0 + tid < nx) {
-        const int k = 2 + tid;
-        const size_t gi = idx2(x0 + tid, o, nx);
-        double az[3], ex[3], ez[3];
+      const int c3 = tid < NT / 2 ? tid : tid - NT / 2;
+      if (c3 < TX && o >= zs && o < ze && x0 + c3 < nx) {
+        const int k = 2 + c3;
+        const size_t gi = idx2(x0 + c3, o, nx);
+        double ex[3], ez[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-          az[a] = sp[(MS_AZ + a) * W + k];
           ex[a] = wk[(MW_EX + rp * 3 + a) * W + k];
           ez[a] = wk[(MW_EZ + a) * W + k];
         }
-        if (!p.freeze_az1) az[0] = az[0] - dt * ez[0];
-        az[1] = az[1] - dt * ez[1];
-        az[2] = az[2] - dt * ez[2];
-        const double kk[3] = {az[1] * ex[2] - az[2] * ex[1], az[2] * ex[0] - az[0] * ex[2],
-                              az[0] * ex[1] - az[1] * ex[0]};
+        if (tid < NT / 2) {
+          double az[3];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          const double dex = (wk[(MW_EX + rq * 3 + a) * W + k] - ex[a]) / p.dz;
-          const double dez = (wk[(MW_EZ + a) * W + k + 1] - ez[a]) / p.dx;
-          out.f[BY1 + a][gi] = sp[(MS_BY + a) * W + k] - dt * (dex - dez - al * kk[a]);
-          out.f[EX1 + a][gi] = ex[a];
-          out.f[EZ1 + a][gi] = ez[a];
-          out.f[AZ1 + a][gi] = az[a];
+          for (int a = 0; a < 3; ++a) az[a] = sp[(MS_AZ + a) * W + k];
+          if (!p.freeze_az1) az[0] = az[0] - dt * ez[0];
+          az[1] = az[1] - dt * ez[1];
+          az[2] = az[2] - dt * ez[2];
+          const double kk[3] = {az[1] * ex[2] - az[2] * ex[1], az[2] * ex[0] - az[0] * ex[2],
+                                az[0] * ex[1] - az[1] * ex[0]};
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const double dex = (wk[(MW_EX + rq * 3 + a) * W + k] - ex[a]) / p.dz;
+            const double dez = (wk[(MW_EZ + a) * W + k + 1] - ez[a]) / p.dx;
+            out.f[BY1 + a][gi] = sp[(MS_BY + a) * W + k] - dt * (dex - dez - al * kk[a]);
+            out.f[AZ1 + a][gi] = az[a];
+          }
+        } else {
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            out.f[EX1 + a][gi] = ex[a];
+            out.f[EZ1 + a][gi] = ez[a];
+          }
         }
       }
     }
