@@ -57,8 +57,12 @@ enum { YMKH_FCT_FUSED = 0, YMKH_FCT_SPLIT = 1 };
 
 /* Filter engines for the periodic-direction DFT mode filter. */
 enum {
-  YMKH_FILTER_DFT = 0    /* dense DFT with the reference's FP32-phase twiddles, FP64 sums
+  YMKH_FILTER_DFT = 0,   /* dense DFT with the reference's FP32-phase twiddles, FP64 sums
                             (ymgpu2d/YM_Physics.cu:349-584) */
+  YMKH_FILTER_TF32X3 = 1 /* the same two contractions on the tensor cores: operands split
+                            into TF32 hi + lo, three passes, FP32 accumulation (a precision
+                            change confined to the subtracted band; NZ a multiple of 128).
+                            No reference counterpart. */
 };
 
 /* GridParams (ymgpu2d/FCT_DeviceMath.cuh:14-17): ny/dy of the reference are

@@ -14,7 +14,7 @@ LIB_PATH = _PKG / "libymkh.so"
 NFIELDS, NFLUID, NSTATE = 12, 6, 24
 MAX_EXTRA_BANDS = 4
 NOALLOC_MAX_CELLS = 134217728  # YMKH_NOALLOC_MAX_CELLS
-FILTER_DFT = 0
+FILTER_DFT, FILTER_TF32X3 = 0, 1
 FCT_FUSED, FCT_SPLIT = 0, 1
 
 # state order of include/ymkh.h

@@ -12,6 +12,9 @@ and the run-length/stride rules of :244-249.
 Extension keys (not in the reference; they never change the step itself):
   ``kz_keep_max = K``   subtract modes (K, NZ/2] every step (keep |k| <= K)
   ``kz_bands = a-b,c-d`` explicit extra subtraction bands
+  ``filter_engine = dft | tf32x3``  how the band filter runs: FP64 sums with
+                        the reference's FP32 twiddles (default), or the
+                        tensor cores with 3-pass split TF32 (NZ % 128 == 0)
 """
 from __future__ import annotations
 
@@ -90,11 +93,14 @@ class RunConfig:
     # extensions
     kz_keep_max: int = -1
     kz_bands: list = field(default_factory=list)
+    filter_engine: str = "dft"
 
+
+FILTER_ENGINES = {"dft": 0, "tf32x3": 1}
 
 _INT_KEYS = {"k_mode", "run_mode", "freeze_override", "suppress_kz0", "kz_suppress_max", "kz_suppress_hi",
              "init_by1_eq", "nz_override", "nx_override", "kz_keep_max"}
-_STR_KEYS = {"run_tag", "seed_profile_file"}
+_STR_KEYS = {"run_tag", "seed_profile_file", "filter_engine"}
 _FLOAT_KEYS = {f.name for f in fields(RunConfig)} - _INT_KEYS - _STR_KEYS - {"kz_bands"}
 
 
@@ -249,7 +255,9 @@ def step_params(cfg: RunConfig, d: Derived | None = None):
     p.n_extra_bands = len(extra)
     for i, (lo, hi) in enumerate(extra):
         p.extra_band_lo[i], p.extra_band_hi[i] = lo, hi
-    p.filter_engine = 0
+    if cfg.filter_engine not in FILTER_ENGINES:
+        raise ConfigError(f"filter_engine must be one of {sorted(FILTER_ENGINES)}, got {cfg.filter_engine!r}")
+    p.filter_engine = FILTER_ENGINES[cfg.filter_engine]
     return p
 
 

@@ -68,6 +68,8 @@ struct ymkh_ctx {
   int nb = 0, lo[MAX_BANDS]{}, hi[MAX_BANDS]{}, J[MAX_BANDS]{};
   double* W[MAX_BANDS]{};
   double* coef = nullptr;    // band coefficients [21][J][nx]
+  Tf32BandImages tfb[MAX_BANDS]{};  // TF32 engine: twiddle tile images per band
+  Tf32Scratch tfs{};                // TF32 engine: G and C^T tile images
   double* epart = nullptr;   // energy partials
   double* edev = nullptr;    // [0] energy, [1..2] mode amplitudes
   double* mcol = nullptr;    // mode amplitude per-column buffer
@@ -124,14 +126,48 @@ void drop_graphs(ymkh_ctx* c) {
 }
 
 void free_bands(ymkh_ctx* c) {
-  for (int b = 0; b < MAX_BANDS; ++b) if (c->W[b]) { cudaFree(c->W[b]); c->W[b] = nullptr; }
+  for (int b = 0; b < MAX_BANDS; ++b) {
+    if (c->W[b]) { cudaFree(c->W[b]); c->W[b] = nullptr; }
+    for (float** q : {&c->tfb[b].a1h, &c->tfb[b].a1l, &c->tfb[b].a2h, &c->tfb[b].a2l})
+      if (*q) { cudaFree(*q); *q = nullptr; }
+  }
+  for (float** q : {&c->tfs.gh, &c->tfs.gl, &c->tfs.ch, &c->tfs.cl})
+    if (*q) { cudaFree(*q); *q = nullptr; }
   if (c->coef) { cudaFree(c->coef); c->coef = nullptr; }
   c->nb = 0;
 }
 
+// TF32 engine set-up: twiddle tile images per band and the shared scratch.
+int setup_tf32(ymkh_ctx* c) {
+  if (c->nz % 128 != 0) return set_err(YMKH_EINVAL, "the TF32X3 filter needs NZ a multiple of 128 (got %d)", c->nz);
+  CK(prepare_tf32(), "TF32 GEMM shared-memory attribute");
+  const size_t tf = tf32_tile_floats();
+  const size_t nt = (size_t)tf32_ntiles(c->nx);
+  int maxJp = 0;
+  for (int b = 0; b < c->nb; ++b) {
+    Tf32BandImages& t = c->tfb[b];
+    t.J = c->J[b];
+    t.Jp = tf32_jpad(c->J[b]);
+    maxJp = std::max(maxJp, t.Jp);
+    const size_t n = (size_t)t.Jp * c->nz;  // floats per image
+    for (float** q : {&t.a1h, &t.a1l, &t.a2h, &t.a2l}) CK(cudaMalloc(q, n * sizeof(float)), "cudaMalloc TF32 twiddle images");
+    CK(launch_tf32_w_images(c->W[b], c->J[b], c->J[b], c->nz, t, 0), "TF32 twiddle images");
+    g_launches++;
+  }
+  const size_t ng = 21 * nt * (size_t)(c->nz / 32) * tf, nc = 21 * nt * (size_t)(maxJp / 32) * tf;
+  CK(cudaMalloc(&c->tfs.gh, ng * sizeof(float)), "cudaMalloc TF32 G images");
+  CK(cudaMalloc(&c->tfs.gl, ng * sizeof(float)), "cudaMalloc TF32 G images");
+  CK(cudaMalloc(&c->tfs.ch, nc * sizeof(float)), "cudaMalloc TF32 coefficient images");
+  CK(cudaMalloc(&c->tfs.cl, nc * sizeof(float)), "cudaMalloc TF32 coefficient images");
+  return 0;
+}
+
 int setup_params(ymkh_ctx* c, const ymkh_params* p) {
   if (p->dt_step <= 0 || p->dx <= 0 || p->dz <= 0) return set_err(YMKH_EINVAL, "dx, dz, dt_step must be > 0");
-  if (p->filter_engine != YMKH_FILTER_DFT) return set_err(YMKH_EINVAL, "unknown filter_engine %d", p->filter_engine);
+  if (p->filter_engine != YMKH_FILTER_DFT && p->filter_engine != YMKH_FILTER_TF32X3)
+    return set_err(YMKH_EINVAL, "unknown filter_engine %d", p->filter_engine);
+  if (p->filter_engine == YMKH_FILTER_TF32X3 && c->nz % 128 != 0)
+    return set_err(YMKH_EINVAL, "the TF32X3 filter needs NZ a multiple of 128 (got %d)", c->nz);
   if (p->suppress_kz0 && (c->nz & (c->nz - 1)) != 0)
     return set_err(YMKH_EINVAL, "suppress_kz0 requires NZ a power of 2 (got %d)", c->nz);
   if (p->n_extra_bands < 0 || p->n_extra_bands > YMKH_MAX_EXTRA_BANDS)
@@ -153,7 +189,12 @@ int setup_params(ymkh_ctx* c, const ymkh_params* p) {
     maxJ = std::max(maxJ, (size_t)c->J[b]);
   }
   c->nb = nb;
-  if (nb) CK(cudaMalloc(&c->coef, 21 * maxJ * (size_t)c->nx * sizeof(double)), "cudaMalloc band coefficients");
+  if (nb && p->filter_engine == YMKH_FILTER_TF32X3) {
+    int rc = setup_tf32(c);
+    if (rc) return rc;
+  } else if (nb) {
+    CK(cudaMalloc(&c->coef, 21 * maxJ * (size_t)c->nx * sizeof(double)), "cudaMalloc band coefficients");
+  }
   CK(cudaDeviceSynchronize(), "twiddle setup");
   return 0;
 }
@@ -285,8 +326,14 @@ int post_stages(ymkh_ctx* c, const State& out, cudaStream_t s) {
   mark(c, ST_BANDS, s);
   const double inv2 = (double)(2.0f / (float)c->nz);
   for (int b = 0; b < c->nb; ++b) {
-    CK(launch_band(list21(out), 21, c->W[b], c->J[b], c->J[b], c->coef, c->nx, c->nz, inv2, s), "band filter");
-    g_launches += 2;
+    if (c->prm.filter_engine == YMKH_FILTER_TF32X3) {
+      CK(launch_band_tf32(list21(out), 21, c->tfb[b], c->tfs, c->nx, c->nz, 2.0f / (float)c->nz, c->derr, s),
+         "band filter (TF32 tensor cores)");
+      g_launches += 3;
+    } else {
+      CK(launch_band(list21(out), 21, c->W[b], c->J[b], c->J[b], c->coef, c->nx, c->nz, inv2, s), "band filter");
+      g_launches += 2;
+    }
   }
   mark(c, ST_HYPER, s);
   if (c->prm.hyp_diff_coeff > 0.0) {

@@ -131,6 +131,25 @@ int energy_nparts(size_t N);
 cudaError_t launch_mode_amp(const double* az2, const double* az3, int nx, int nz, int k, double* colbuf, double* out,
                             cudaStream_t s);
 cudaError_t launch_init(const State& st, const InitArgs& a, cudaStream_t s);
+// 3-pass TF32 band filter on the tensor cores (ymkh_tf32.cu).  Per band:
+// the twiddle matrix as TF32 hi/lo tile images for both contractions;
+// shared scratch: the G and C^T tile images of the filtered arrays.
+struct Tf32BandImages {
+  float *a1h, *a1l;  // rows j, k = z: [Jp/128][NZ/32] tiles
+  float *a2h, *a2l;  // rows z, k = j: [NZ/128][Jp/32] tiles
+  int J, Jp;
+};
+struct Tf32Scratch {
+  float *gh, *gl;    // [narr][NT][NZ/32] tiles
+  float *ch, *cl;    // [narr][NT][Jp/32] tiles
+};
+int tf32_ntiles(int nx);
+int tf32_jpad(int J);
+size_t tf32_tile_floats();
+cudaError_t prepare_tf32();
+cudaError_t launch_tf32_w_images(const double* W, int ldw, int J, int nz, const Tf32BandImages& b, cudaStream_t s);
+cudaError_t launch_band_tf32(const ArrayList& arrs, int narr, const Tf32BandImages& b, const Tf32Scratch& w, int nx,
+                             int nz, float inv2, unsigned* err, cudaStream_t s);
 int capi_error(int code, const char* msg);
 void capi_count_launches(int n);
 

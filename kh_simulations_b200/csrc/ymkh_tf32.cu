@@ -1,0 +1,379 @@
+// ymkh_tf32.cu — the DFT band filter on the 5th-generation tensor cores:
+// split-precision 3-pass TF32 with FP32 accumulation in tensor memory.
+//
+// The band filter of ymgpu2d/YM_Physics.cu:349-584 (per column x, for each
+// subtracted mode m: A_m = inv2 sum_z v cos, B_m = inv2 sum_z v sin, then
+// v -= sum_m (A_m cos + B_m sin)) is, over all 21 filtered arrays, two
+// contractions per array k with the twiddle matrix W[z, j] (j = 2(m-lo) for
+// cos, +1 for sin; the reference's FP32-phase twiddles):
+//   GEMM 1:  C[j, x] = inv2 * sum_z W[z, j] G[z, x]      M = J, N = NX, K = NZ
+//   GEMM 2:  G[z, x] -= sum_j W[z, j] C[j, x]            M = NZ, N = NX, K = J
+// Here both run as tcgen05.mma kind::tf32 (M = N = 128 tiles, K = 8 per
+// instruction) with every FP32/FP64 operand split as x ~ hi + lo, hi and lo
+// TF32 (round to nearest), and the product formed as
+//   lo_a*hi_b + hi_a*lo_b + hi_a*hi_b        (three passes, FP32 accumulate)
+// which keeps ~2^-22 relative error per product against 2^-11 for one pass.
+// The FP64 state is only read and written in FP64; the precision change is
+// confined to the subtracted band content.
+//
+// Operand layout.  Every operand tile is 128 rows x 32 TF32 (K) = 16 KB, in
+// the K-major 128-byte-swizzled layout the tensor core reads (8-row groups
+// of 1024 B; 16-byte chunk index XOR row % 8).  The split kernels write
+// whole tile images to global memory, so the GEMM stages each tile with one
+// 16 KB TMA bulk copy (cp.async.bulk) and no tensor map:
+//   W images  (built once per band):  A1 [mt = j/128][kt = z/32]   A2 [mt = z/128][kt = j/32]
+//   G image   (per step, per array):   [array][nt = x/128][kt = z/32]      (B of GEMM 1)
+//   C^T image (GEMM 1's epilogue):     [array][nt = x/128][kt = j/32]      (B of GEMM 2)
+// Rows beyond J or NX are zero.  NZ must be a multiple of 128.
+//
+// Pipeline per CTA (128 threads, one 128x128 output tile): thread 0 issues
+// the bulk copies of a 3-stage ring (A hi/lo + B hi/lo per stage) on "full"
+// mbarriers; thread 32 waits for a stage, issues its 12 MMAs and commits
+// them to the stage's "empty" mbarrier; after the last stage it commits to
+// "done", and the four warps read the accumulator out of tensor memory
+// (tcgen05.ld, warp w owns lanes 32w..32w+31) for the epilogue.  GEMM 1's
+// epilogue writes the split coefficients straight into the C^T image (a
+// warp covers one 128-byte tile row); GEMM 2's stages the tile in the idle
+// operand buffers and updates G row by row with the CTA's threads on
+// consecutive x (coalesced FP64 read-modify-write).  Every mbarrier wait is
+// bounded and reports through the device error word.
+
+#include "ymkh_common.cuh"
+
+namespace ymkh {
+
+namespace {
+
+constexpr int TT_M = 128;                 // tile rows (UMMA M)
+constexpr int TT_N = 128;                 // tile columns (UMMA N)
+constexpr int TT_K = 32;                  // K per tile: one 128-byte swizzle row of TF32
+constexpr int TT_BYTES = TT_M * TT_K * 4; // 16 KB tile image
+constexpr int TT_FLOATS = TT_BYTES / 4;
+constexpr int TT_NS = 3;                  // pipeline stages, 4 tiles each
+constexpr int TT_THREADS = 128;
+constexpr size_t TT_SMEM = (size_t)TT_NS * 4 * TT_BYTES + 1024;  // + alignment slack
+constexpr uint32_t TT_TMEM_COLS = 128;    // FP32 accumulator 128 lanes x 128 columns
+
+// instruction descriptor, kind::tf32: D F32 (bits 4-5 = 1), A and B TF32
+// (bits 7-9, 10-12 = 2), both K-major (bits 15, 16 = 0), N >> 3 at bit 17,
+// M >> 4 at bit 24
+constexpr uint32_t kIdescTF32 =
+    (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TT_N >> 3) << 17) | ((uint32_t)(TT_M >> 4) << 24);
+
+// byte offset of element (row r, k-column c) in a 128 x 32 TF32 tile image
+__host__ __device__ __forceinline__ unsigned tile_off(int r, int c) {
+  return (unsigned)((r >> 3) * 1024 + (r & 7) * 128 + ((((c >> 2) ^ (r & 7)) & 7) << 4) + (c & 3) * 4);
+}
+
+__device__ __forceinline__ float tf32_rna(float v) {
+  unsigned u;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(v));
+  return __uint_as_float(u);
+}
+
+__device__ __forceinline__ void split_f32(float f, float& hi, float& lo) {
+  hi = tf32_rna(f);
+  lo = tf32_rna(f - hi);  // exact difference: hi is f rounded at mantissa bit 13
+}
+
+__device__ __forceinline__ void split_f64(double g, float& hi, float& lo) {
+  hi = tf32_rna((float)g);
+  lo = tf32_rna((float)(g - (double)hi));
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: K-major, 128-byte swizzle; start >> 4 in
+// bits 0-13, leading byte offset 16 B (unused for this layout) in 16-29,
+// stride byte offset 1024 B (next 8-row group) in 32-45, descriptor version
+// 1 in 46-47, swizzle mode 2 (128 B) in 61-63
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+        "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// ---- split kernels ------------------------------------------------------
+
+// W[z * ldw + j] (FP64 holding the FP32 twiddles) -> A1 (rows j, k = z) and
+// A2 (rows z, k = j) tile images, hi and lo; j in [J, Jp) is zero.
+__global__ void w_image_kernel(const double* __restrict__ W, int ldw, int J, int Jp, int nz, float* __restrict__ a1h,
+                               float* __restrict__ a1l, float* __restrict__ a2h, float* __restrict__ a2l) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int z = blockIdx.y;
+  if (j >= Jp || z >= nz) return;
+  const float w = (j < J) ? (float)W[(size_t)z * ldw + j] : 0.0f;
+  float hi, lo;
+  split_f32(w, hi, lo);
+  const int kt1 = nz / TT_K, kt2 = Jp / TT_K;
+  const size_t t1 = ((size_t)(j / TT_M) * kt1 + z / TT_K) * TT_FLOATS + (tile_off(j % TT_M, z % TT_K) >> 2);
+  const size_t t2 = ((size_t)(z / TT_M) * kt2 + j / TT_K) * TT_FLOATS + (tile_off(z % TT_M, j % TT_K) >> 2);
+  a1h[t1] = hi;
+  a1l[t1] = lo;
+  a2h[t2] = hi;
+  a2l[t2] = lo;
+}
+
+// G_k[z, x] (FP64) -> B image of GEMM 1, tile (nt, kt) of array k: rows x,
+// k = z.  Coalesced reads along x; the swizzled tile is assembled in shared
+// memory and written out linearly.
+__global__ void __launch_bounds__(256)
+    g_image_kernel(const __grid_constant__ ArrayList arrs, int nx, int NT, int KT, float* __restrict__ gh,
+                   float* __restrict__ gl) {
+  __shared__ __align__(16) float sh[TT_FLOATS];
+  __shared__ __align__(16) float sl[TT_FLOATS];
+  const int nt = blockIdx.x, kt = blockIdx.y, k = blockIdx.z;
+  const double* G = arrs.p[k];
+  for (int i = threadIdx.x; i < TT_K * TT_N; i += 256) {
+    const int zz = i / TT_N, xx = i - zz * TT_N;
+    const int x = nt * TT_N + xx, z = kt * TT_K + zz;
+    const double g = (x < nx) ? G[(size_t)z * nx + x] : 0.0;
+    float hi, lo;
+    split_f64(g, hi, lo);
+    const unsigned o = tile_off(xx, zz) >> 2;
+    sh[o] = hi;
+    sl[o] = lo;
+  }
+  __syncthreads();
+  const size_t t = (((size_t)k * NT + nt) * KT + kt) * TT_FLOATS;
+  float4* dh = reinterpret_cast<float4*>(gh + t);
+  float4* dl = reinterpret_cast<float4*>(gl + t);
+  for (int i = threadIdx.x; i < TT_FLOATS / 4; i += 256) {
+    dh[i] = reinterpret_cast<const float4*>(sh)[i];
+    dl[i] = reinterpret_cast<const float4*>(sl)[i];
+  }
+}
+
+// ---- the GEMM -----------------------------------------------------------
+
+struct Tf32GemmArgs {
+  const float* a_hi;  // A tile images [mt][KT]
+  const float* a_lo;
+  const float* b_hi;  // B tile images [array][nt][KT]
+  const float* b_lo;
+  int KT;             // K tiles
+  int NT;             // N tiles per array
+  // EPI_COEF: C^T image out, [array][nt][KT2] tiles (rows x, k = j)
+  float* c_hi;
+  float* c_lo;
+  int KT2;
+  float scale;
+  // EPI_APPLY: G_k[z, x] -= D[z, x]
+  ArrayList arrs;
+  int nx;
+  unsigned* err;
+};
+
+constexpr int EPI_COEF = 0, EPI_APPLY = 1;
+
+template <int EPI>
+__global__ void __launch_bounds__(TT_THREADS, 1) tf32x3_gemm_kernel(const __grid_constant__ Tf32GemmArgs g) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* const smem =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  __shared__ __align__(8) uint64_t full[TT_NS];
+  __shared__ __align__(8) uint64_t empty[TT_NS];
+  __shared__ __align__(8) uint64_t done;
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nt = blockIdx.x, mt = blockIdx.y, k = blockIdx.z;
+  const int KT = g.KT;
+
+  if (tid == 0) {
+    for (int s = 0; s < TT_NS; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(&done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(TT_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base;
+
+  const float* const A_hi = g.a_hi + (size_t)mt * KT * TT_FLOATS;
+  const float* const A_lo = g.a_lo + (size_t)mt * KT * TT_FLOATS;
+  const size_t bt = ((size_t)k * g.NT + nt) * KT * TT_FLOATS;
+  const float* const B_hi = g.b_hi + bt;
+  const float* const B_lo = g.b_lo + bt;
+
+  if (warp == 0 && lane == 0) {
+    // producer: four 16 KB tile copies per stage
+    for (int kt = 0; kt < KT; ++kt) {
+      const int s = kt % TT_NS, u = kt / TT_NS;
+      if (u > 0) mbar_wait(&empty[s], (unsigned)((u - 1) & 1), g.err);
+      unsigned char* const st = smem + (size_t)s * 4 * TT_BYTES;
+      mbar_expect_tx(&full[s], 4u * TT_BYTES);
+      const size_t o = (size_t)kt * TT_FLOATS;
+      bulk_g2s(st, A_hi + o, TT_BYTES, &full[s]);
+      bulk_g2s(st + TT_BYTES, A_lo + o, TT_BYTES, &full[s]);
+      bulk_g2s(st + 2 * TT_BYTES, B_hi + o, TT_BYTES, &full[s]);
+      bulk_g2s(st + 3 * TT_BYTES, B_lo + o, TT_BYTES, &full[s]);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer: per stage and K step of 8, lo*hi + hi*lo + hi*hi
+    for (int kt = 0; kt < KT; ++kt) {
+      const int s = kt % TT_NS, u = kt / TT_NS;
+      mbar_wait(&full[s], (unsigned)(u & 1), g.err);
+      tc_fence_after();
+      const uint32_t st = smem_u32(smem + (size_t)s * 4 * TT_BYTES);
+#pragma unroll
+      for (int kk = 0; kk < TT_K / 8; ++kk) {
+        const uint32_t off = (uint32_t)kk * 32u;  // 8 TF32 = 32 bytes along the swizzled row
+        const uint64_t ah = sw128_desc(st + off), al = sw128_desc(st + TT_BYTES + off);
+        const uint64_t bh = sw128_desc(st + 2 * TT_BYTES + off), bl = sw128_desc(st + 3 * TT_BYTES + off);
+        umma_tf32(tmem, al, bh, kIdescTF32, (kt | kk) != 0 ? 1u : 0u);
+        umma_tf32(tmem, ah, bl, kIdescTF32, 1u);
+        umma_tf32(tmem, ah, bh, kIdescTF32, 1u);
+      }
+      umma_commit(&empty[s]);  // stage s free once these MMAs have read it
+    }
+    umma_commit(&done);
+  }
+  __syncwarp();
+
+  // epilogue: warp w reads TMEM lanes 32w..32w+31 = tile rows
+  mbar_wait(&done, 0u, g.err);
+  __syncwarp();
+  tc_fence_after();
+  const int row = mt * TT_M + 32 * warp + lane;
+  // EPI_APPLY stages the tile in the (now idle) operand buffers as
+  // [128][129] floats (row padding: conflict-free both ways)
+  float* const dtile = reinterpret_cast<float*>(smem);
+#pragma unroll 1
+  for (int cc = 0; cc < TT_N; cc += 32) {
+    uint32_t v[32];
+    tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)cc, v);
+    if (EPI == EPI_COEF) {
+      // row = j; columns x = nt*128 + cc + i -> C^T image tile (nt, j/32),
+      // tile row cc + i, k-column j % 32 = lane: one 128-byte row per warp
+      const size_t t = (((size_t)k * g.NT + nt) * g.KT2 + (row >> 5)) * TT_FLOATS;
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        float hi, lo;
+        split_f32(__uint_as_float(v[i]) * g.scale, hi, lo);
+        const unsigned o = tile_off(cc + i, lane) >> 2;
+        g.c_hi[t + o] = hi;
+        g.c_lo[t + o] = lo;
+      }
+    } else {
+      const int r = 32 * warp + lane;
+#pragma unroll
+      for (int i = 0; i < 32; ++i) dtile[r * (TT_N + 1) + cc + i] = __uint_as_float(v[i]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (EPI == EPI_APPLY) {
+    // G_k[z, x] -= D[z, x]: one tile row at a time, thread = column (coalesced)
+    // (16 rows loaded before any is stored, so the loads overlap)
+    const int x = nt * TT_N + tid;
+    if (x < g.nx) {
+      double* const G = g.arrs.p[k] + (size_t)mt * TT_M * g.nx + x;
+      const size_t ld = (size_t)g.nx;
+#pragma unroll 1
+      for (int r0 = 0; r0 < TT_M; r0 += 16) {
+        double gv[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) gv[i] = G[(size_t)(r0 + i) * ld];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) G[(size_t)(r0 + i) * ld] = gv[i] - (double)dtile[(r0 + i) * (TT_N + 1) + tid];
+      }
+    }
+  }
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TT_TMEM_COLS));
+  }
+}
+
+}  // namespace
+
+int tf32_ntiles(int nx) { return (nx + TT_N - 1) / TT_N; }
+int tf32_jpad(int J) { return ((J + TT_M - 1) / TT_M) * TT_M; }
+size_t tf32_tile_floats() { return TT_FLOATS; }
+
+cudaError_t prepare_tf32() {
+  cudaError_t e = cudaFuncSetAttribute(tf32x3_gemm_kernel<EPI_COEF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)TT_SMEM);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(tf32x3_gemm_kernel<EPI_APPLY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)TT_SMEM);
+}
+
+cudaError_t launch_tf32_w_images(const double* W, int ldw, int J, int nz, const Tf32BandImages& b, cudaStream_t s) {
+  if (nz % TT_M != 0) return cudaErrorInvalidValue;
+  dim3 grid((b.Jp + 127) / 128, nz);
+  w_image_kernel<<<grid, 128, 0, s>>>(W, ldw, J, b.Jp, nz, b.a1h, b.a1l, b.a2h, b.a2l);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_band_tf32(const ArrayList& arrs, int narr, const Tf32BandImages& b, const Tf32Scratch& w, int nx,
+                             int nz, float inv2, unsigned* err, cudaStream_t s) {
+  if (nz % TT_M != 0 || narr < 1) return cudaErrorInvalidValue;
+  const int NT = tf32_ntiles(nx), KT1 = nz / TT_K, MT1 = b.Jp / TT_M, KT2 = b.Jp / TT_K, MT2 = nz / TT_M;
+  g_image_kernel<<<dim3(NT, KT1, narr), 256, 0, s>>>(arrs, nx, NT, KT1, w.gh, w.gl);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  Tf32GemmArgs g1{};
+  g1.a_hi = b.a1h;
+  g1.a_lo = b.a1l;
+  g1.b_hi = w.gh;
+  g1.b_lo = w.gl;
+  g1.KT = KT1;
+  g1.NT = NT;
+  g1.c_hi = w.ch;
+  g1.c_lo = w.cl;
+  g1.KT2 = KT2;
+  g1.scale = inv2;
+  g1.arrs = arrs;
+  g1.nx = nx;
+  g1.err = err;
+  tf32x3_gemm_kernel<EPI_COEF><<<dim3(NT, MT1, narr), TT_THREADS, TT_SMEM, s>>>(g1);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  Tf32GemmArgs g2 = g1;
+  g2.a_hi = b.a2h;
+  g2.a_lo = b.a2l;
+  g2.b_hi = w.ch;
+  g2.b_lo = w.cl;
+  g2.KT = KT2;
+  tf32x3_gemm_kernel<EPI_APPLY><<<dim3(NT, MT2, narr), TT_THREADS, TT_SMEM, s>>>(g2);
+  return cudaGetLastError();
+}
+
+}  // namespace ymkh
