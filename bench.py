@@ -227,6 +227,9 @@ def main() -> int:
     ap.add_argument("--with-filter-line", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-filter-leg", action="store_true", help="skip the FP64 vs TF32 band filter leg")
+    ap.add_argument("--filter-error-steps", type=int, default=0, help="steps of the TF32-vs-FP64 filter error leg")
+    ap.add_argument("--filter-error-runs", type=int, default=2)
     ap.add_argument("--batched-runs", type=int, default=64, help="runs in the batched-vs-plain leg (0: skip)")
     ap.add_argument("--served-seconds", type=float, default=3.0, help="arrival window of the served leg (0: skip)")
     args = ap.parse_args()
@@ -321,6 +324,10 @@ def main() -> int:
 
     if args.with_filter_line and args.filter == "ref" and d.nz > 1024:
         line["filter_keep"] = filter_keep_rate(args, dev)
+    if world == 1 and not args.no_filter_leg:
+        line["filter"] = filter_engines(args, dev)
+    if world == 1 and args.filter_error_steps > 0:
+        line["filter_error"] = filter_error(args, dev, args.filter_error_steps, args.filter_error_runs)
     if world == 1 and args.batched_runs > 0:
         line["batched"] = batched_rate(args, dev, args.batched_runs)
     if world == 1 and args.served_seconds > 0:
@@ -467,6 +474,126 @@ def served_rate(args, dev, seconds: float) -> dict:
             "served": {k: a[k] for k in keys}, "sequential": {k: b[k] for k in keys},
             "served_over_sequential": a["cell_steps_per_s"] / b["cell_steps_per_s"] if b["cell_steps_per_s"] else None,
             "max_rel_energy_diff": de, "unit": "cell-steps/s", "latency_clock": "host wall clock (arrival to completion)"}
+
+
+def measured_tf32_peak() -> tuple:
+    """TF32 dense tensor rate: half the measured bf16 dense burst rate (the
+    B200's TF32 rate is half its bf16 rate); nominal 1.1 PFLOP/s otherwise."""
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        if "bf16_tflops" in d:
+            return float(d["bf16_tflops"]) / 2.0, "half of measured bf16 dense"
+    return 1100.0, "nominal"
+
+
+def filter_engines(args, dev) -> dict:
+    """The DFT band filter at the split-precision configuration's size (one
+    run at NZ 1024 x NX 2048, keep |k| <= NZ/3: modes 342..512 subtracted, 21
+    arrays): band-stage device time with the FP64 filter and with the 3-pass
+    TF32 tensor-core filter, the step time with each, and the tensor
+    roofline of the TF32 filter."""
+    import torch
+
+    from kh_simulations_b200 import _lib
+    from kh_simulations_b200.config import loads
+    from kh_simulations_b200.run import KHRun
+
+    wl = "kh_1024x2048"
+    out = {"workload": f"{wl}, keep |k| <= NZ/3, 21 filtered arrays", "bands_ms": {}, "step_ms": {}}
+    lib = _lib.load()
+    bands = None
+    for eng in ("dft", "tf32x3"):
+        run = KHRun(loads(ini_for(wl, "keep") + f"filter_engine = {eng}\n"), device=dev)
+        run.init()
+        stream = torch.cuda.Stream(device=dev)
+        t = (C.c_float * 8)()
+        _lib.check(lib.ymkh_stage_times(run.ctx, 3, C.c_void_p(stream.cuda_stream), t, 8), "stage times")
+        n = 10
+        _lib.check(lib.ymkh_stage_times(run.ctx, n, C.c_void_p(stream.cuda_stream), t, 8), "stage times")
+        out["bands_ms"][eng] = t[4] / n
+        out["step_ms"][eng] = sum(t[:7]) / n
+        bands = run.d.bands
+        nx, nz = run.d.nx, run.d.nz
+        run.close()
+    # algorithmic flops of the two contractions per band and array
+    flops = sum(2 * 2.0 * (2 * (hi - lo + 1)) * nx * nz * 21 for lo, hi in bands)
+    peak, kind = measured_tf32_peak()
+    ms = out["bands_ms"]["tf32x3"]
+    achieved = flops / (ms / 1e3) / 1e12
+    out["speedup_tf32x3_over_dft"] = out["bands_ms"]["dft"] / ms
+    out["roofline_tf32x3"] = {"bound": "tensor", "achieved": achieved, "executed": 3 * achieved, "peak": peak,
+                              "unit": "TFLOP/s", "frac": 3 * achieved / peak, "peak_source": kind,
+                              "note": "achieved = algorithmic flops / band-stage time; executed counts the 3 passes"}
+    return out
+
+
+def filter_error(args, dev, steps: int, nruns: int) -> dict:
+    """Error of the 3-pass TF32 filter against the FP64 filter, from the same
+    initial state, on `nruns` runs at NZ 1024 x NX 2048 (seed 2,
+    uneven-sweep parameter ranges, keep |k| <= NZ/3).  Both engines step in
+    lockstep in chunks of 100 until `steps` or until either meets the
+    reference's halt rule (NaN/Inf or E/E0 above the threshold,
+    ymgpu2d/main_ym.cu:467-474); the per-field relative L2 of the state and
+    the relative error of the k_mode amplitude are taken at the last chunk
+    both completed."""
+    import math
+
+    import numpy as np
+    import torch
+
+    from kh_simulations_b200._lib import STATE_NAMES
+    from kh_simulations_b200.run import KHRun
+    from kh_simulations_b200.server import split_precision_runs
+
+    # groups of arrays sharing a scale (E, By, Az, n, p, Q of each beam): an
+    # array's error is divided by its group's largest norm, as in the parity
+    # tests (some arrays are pure cancellation residues beside their group)
+    groups = [range(0, 6), range(6, 9), range(9, 12), [12], [13, 14], range(15, 18), [18], [19, 20], range(21, 24)]
+    checkpoints = sorted({c for c in (1, 100, 1000, 2000, steps) if c <= steps})
+    table = {c: np.zeros(24) for c in checkpoints}
+    amp = {c: 0.0 for c in checkpoints}
+    reached = []
+    for cfg in split_precision_runs(2, nruns, SWEEP_BASE):
+        runs = {}
+        for eng in ("dft", "tf32x3"):
+            cfg.filter_engine = eng
+            r = KHRun(cfg, device=dev)
+            r.init()
+            r.E0 = r.energy()
+            runs[eng] = r
+        done = 0
+        for c in checkpoints:
+            k = c - done
+            ok = True
+            while k > 0 and ok:
+                kk = min(100, k)
+                for r in runs.values():
+                    r.step(kk)
+                    e = r.energy()
+                    ok = ok and math.isfinite(e) and e / r.E0 <= r.d.energy_thresh
+                k -= kk
+            if not ok:
+                break
+            done = c
+            a, b = runs["tf32x3"].state, runs["dft"].state
+            d = (a - b).reshape(24, -1).norm(dim=1).cpu().numpy()
+            n = b.reshape(24, -1).norm(dim=1).cpu().numpy()
+            for g in groups:
+                g = list(g)
+                scale = max(n[g].max(), 1e-300)
+                table[c][g] = np.maximum(table[c][g], d[g] / scale)
+            ma, mb = runs["tf32x3"].mode_amp()[0], runs["dft"].mode_amp()[0]
+            amp[c] = max(amp[c], abs(ma - mb) / max(abs(mb), 1e-300))
+        reached.append(done)
+        for r in runs.values():
+            r.close()
+        torch.cuda.empty_cache()
+    return {"workload": f"{nruns} runs at 1024x2048 (seed 2), keep |k| <= NZ/3, up to {steps} steps",
+            "steps_reached": reached, "metric": "per-array rel-L2, divided by the largest norm in its group",
+            "max_rel_l2_by_step": {str(c): {STATE_NAMES[i]: float(table[c][i]) for i in range(24)} for c in checkpoints},
+            "max_rel_mode_amp_err_by_step": {str(c): amp[c] for c in checkpoints},
+            "reference": "the FP64 filter (matches the oracle to 1e-12 per step)"}
 
 
 def filter_keep_rate(args, dev) -> dict:

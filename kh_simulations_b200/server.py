@@ -315,3 +315,22 @@ def uneven_sweep(seed: int, n: int, base_ini: str = "") -> list:
         out.append(loads(ini, f"sweep{i}"))
     return out
 
+
+def split_precision_runs(seed: int, n: int, base_ini: str = "", nz: int = 1024, nx: int = 2048) -> list:
+    """n runs at NZ x NX with the uneven sweep's parameter ranges (seed `seed`)
+    and the band filter keeping |k| <= NZ/3."""
+    from .config import loads
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        v0 = rng.uniform(0.02, 0.2)
+        eps = rng.uniform(0.5, 2.0)
+        kz = int(rng.integers(0, 4))
+        amp = rng.uniform(0.05, 0.2)
+        ini = (base_ini + f"k_mode = {kz}\nV0 = {v0:.6f}\neps_override = {eps:.6f}\nperturb_amp = {amp:.6f}\n"
+               f"nz_override = {nz}\nnx_override = {nx}\ncourant_override = {cfl_courant(nx, nz):.6f}\n"
+               f"suppress_kz0 = {1 if i % 2 == 0 else 0}\nkz_keep_max = {nz // 3}\n")
+        out.append(loads(ini, f"split{i}"))
+    return out
+
