@@ -49,9 +49,9 @@ BYTES_FCT = 288   # fct_fused_kernel: read 12 fluid + 12 field arrays, write 12 
 BYTES_MAXWELL = 280  # maxwell_fused_kernel: read 24, write 11 (Az1 frozen)
 
 
-def ini_for(workload: str, filt: str) -> str:
+def ini_for(workload: str, filt: str, engine: str = "dft") -> str:
     nx, nz = WORKLOADS[workload]
-    text = PHYSICS + f"nx_override = {nx}\nnz_override = {nz}\n"
+    text = PHYSICS + f"nx_override = {nx}\nnz_override = {nz}\nfilter_engine = {engine}\n"
     if filt == "keep" or (filt == "ref" and nz <= 1024):
         text += f"kz_keep_max = {nz // 3}\n"
     return text
@@ -224,6 +224,8 @@ def main() -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="kh_4096x8192")
     ap.add_argument("--filter", choices=["ref", "keep"], default="ref")
+    ap.add_argument("--filter-engine", choices=["dft", "tf32x3"], default="dft",
+                    help="band filter of the main run: FP64 sums or 3-pass TF32 on the tensor cores")
     ap.add_argument("--with-filter-line", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -254,7 +256,7 @@ def main() -> int:
 
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
-    cfg = loads(ini_for(args.workload, args.filter))
+    cfg = loads(ini_for(args.workload, args.filter, args.filter_engine))
     run = KHRun(cfg, device=dev)
     run.init()
     d = run.d
@@ -504,7 +506,7 @@ def filter_engines(args, dev) -> dict:
     lib = _lib.load()
     bands = None
     for eng in ("dft", "tf32x3"):
-        run = KHRun(loads(ini_for(wl, "keep") + f"filter_engine = {eng}\n"), device=dev)
+        run = KHRun(loads(ini_for(wl, "keep", eng)), device=dev)
         run.init()
         stream = torch.cuda.Stream(device=dev)
         t = (C.c_float * 8)()
