@@ -63,13 +63,15 @@ __device__ __forceinline__ void beam_bar(int group, int nthreads) {
 }
 
 // apply_fct_limiter (FCT_DeviceMath.cuh:108-125) with the products by
-// copysign(1, d0) written as sign selections, which give the same values.
+// copysign(1, d0) written as flips of the sign bit: multiplying by -1 is an
+// exact negation, i.e. the same bits.
+__device__ __forceinline__ double flip_sign(double x, unsigned long long m) {
+  return __longlong_as_double(__double_as_longlong(x) ^ m);
+}
 __device__ __forceinline__ double fct_limit_sel(double f, double dm1, double d0, double dp1) {
-  const bool neg = signbit(d0);
-  const double term = neg ? -dm1 : dm1;
-  const double terp = neg ? -dp1 : dp1;
-  const double r = fmax(0.0, fmin(term, fmin(fabs(f), terp)));
-  return neg ? -r : r;
+  const unsigned long long m = (unsigned long long)__double_as_longlong(d0) & 0x8000000000000000ull;
+  const double r = fmax(0.0, fmin(flip_sign(dm1, m), fmin(fabs(f), flip_sign(dp1, m))));
+  return flip_sign(r, m);
 }
 
 }  // namespace
@@ -148,6 +150,34 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
     for (int i = tid; i < 2 * 2 * W; i += NT) wk[(size_t)(i / (2 * W)) * WB_SIZE * W + WB_SZ * W + i % (2 * W)] = 0.0;
     __syncthreads();
 
+    // LOAD_BULK_ALL: this thread's row copy for the item (array a of the
+    // stage, lane-major over the warps): source array, stage slot, which row
+    // (0: z, 1: z-1, 2: z+1) and the split at the periodic wrap
+    const double* cp_base = nullptr;
+    int cp_dst = 0, cp_kind = 0, cp_x1 = 0, cp_len1 = W;
+    if (lmode == LOAD_BULK_ALL) {
+      const int a = (tid & 31) * (NT / 32) + (tid >> 5);
+      if (a < 33 + (warm ? 4 : 0)) {
+        if (a < 12) {
+          cp_base = a < 6 ? st.a[a] : st.b[a - 6];
+          cp_dst = ST_FL + a;
+        } else if (a < 33) {
+          const int kind = (a - 12) / 3, c = (a - 12) - kind * 3;  // EX, BY, BYM, EZ, EZM, AZ, AZM
+          cp_base = (kind == 0) ? st.f[EX1 + c] : (kind <= 2) ? st.f[BY1 + c] : (kind <= 4) ? st.f[EZ1 + c] : st.f[AZ1 + c];
+          cp_dst = ST_EX + (a - 12);
+          cp_kind = (kind == 2 || kind == 4 || kind == 6) ? 1 : 0;
+        } else {
+          const int w = a - 33;  // NZP A, NZP B, NZM A, NZM B
+          cp_base = (w & 1) ? st.b[FN] : st.a[FN];
+          cp_dst = ST_NZP + w;
+          cp_kind = (w >> 1) ? 1 : 2;
+        }
+        int x = (x0 - 4) % nx;
+        cp_x1 = x < 0 ? x + nx : x;
+        cp_len1 = min(W, nx - cp_x1);
+      }
+    }
+
     auto issue_row = [&](int r) {
       const int s = (int)(issued % NST);
       double* sb = stage + (size_t)s * ST_SIZE * W;
@@ -190,13 +220,14 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
         // one row copy per thread, spread over the warps (lane-major) so no
         // single warp serialises the issue; completions that land before
         // thread 0 arms the stage only drive its transaction count negative,
-        // and the phase cannot complete before that arrival
+        // and the phase cannot complete before that arrival.  The copy's
+        // array, slot and wrap split are fixed per item (cp_*).
         if (tid == 0) mbar_expect_tx(&bars[s], (unsigned)(narr * W * 8));
-        const int a = (tid & 31) * (NT / 32) + (tid >> 5);
-        if (a < narr) {
-          int dsto;
-          const double* row = row_src(a, dsto);
-          bulk_row_periodic(sb + dsto * W, row, xs, W, nx, &bars[s]);
+        if (cp_base) {
+          const size_t off = cp_kind == 0 ? ro : (cp_kind == 1 ? rom : rop);
+          double* const dst = sb + cp_dst * W;
+          bulk_g2s(dst, cp_base + off + cp_x1, (unsigned)cp_len1 * 8u, &bars[s]);
+          if (cp_len1 < W) bulk_g2s(dst + cp_len1, cp_base + off, (unsigned)(W - cp_len1) * 8u, &bars[s]);
         }
       } else if (lmode == LOAD_VEC16) {
         // 16-byte chunks (x even, nx even and >= W: a chunk never straddles

@@ -27,12 +27,15 @@ namespace {
 constexpr int XT = 64;        // x-sweep positions per CTA (per beam)
 constexpr int XO = XT - 6;    // x-swept columns produced per CTA
 
+// apply_fct_limiter (FCT_DeviceMath.cuh:108-125); the products by
+// copysign(1, d0) are sign-bit flips (multiplying by -1 negates exactly)
+__device__ __forceinline__ double flip_sign2(double x, unsigned long long m) {
+  return __longlong_as_double(__double_as_longlong(x) ^ m);
+}
 __device__ __forceinline__ double fct_limit_sel2(double f, double dm1, double d0, double dp1) {
-  const bool neg = signbit(d0);
-  const double term = neg ? -dm1 : dm1;
-  const double terp = neg ? -dp1 : dp1;
-  const double r = fmax(0.0, fmin(term, fmin(fabs(f), terp)));
-  return neg ? -r : r;
+  const unsigned long long m = (unsigned long long)__double_as_longlong(d0) & 0x8000000000000000ull;
+  const double r = fmax(0.0, fmin(flip_sign2(dm1, m), fmin(fabs(f), flip_sign2(dp1, m))));
+  return flip_sign2(r, m);
 }
 
 }  // namespace
