@@ -26,17 +26,12 @@
 //   C^T image (GEMM 1's epilogue):     [array][nt = x/128][kt = j/32]      (B of GEMM 2)
 // Rows beyond J or NX are zero.  NZ must be a multiple of 128.
 //
-// Pipeline per CTA (128 threads, one 128x128 output tile): thread 0 issues
-// the bulk copies of a 3-stage ring (A hi/lo + B hi/lo per stage) on "full"
-// mbarriers; thread 32 waits for a stage, issues its 12 MMAs and commits
-// them to the stage's "empty" mbarrier; after the last stage it commits to
-// "done", and the four warps read the accumulator out of tensor memory
-// (tcgen05.ld, warp w owns lanes 32w..32w+31) for the epilogue.  GEMM 1's
-// epilogue writes the split coefficients straight into the C^T image (a
-// warp covers one 128-byte tile row); GEMM 2's stages the tile in the idle
-// operand buffers and updates G row by row with the CTA's threads on
-// consecutive x (coalesced FP64 read-modify-write).  Every mbarrier wait is
-// bounded and reports through the device error word.
+// The GEMM kernel is persistent and warp-specialised (see tf32x3_gemm_ws):
+// a producer lane streams operand tiles through a 3-stage ring of "full" /
+// "empty" mbarriers, an MMA lane issues 12 MMAs per stage into one of two
+// TMEM accumulators, and four epilogue warps drain the other one, so the
+// epilogue of a tile overlaps the main loop of the next.  Every mbarrier
+// wait is bounded and reports through the device error word.
 
 #include "ymkh_common.cuh"
 
@@ -45,20 +40,14 @@ namespace ymkh {
 namespace {
 
 constexpr int TT_M = 128;                 // tile rows (UMMA M)
-constexpr int TT_N = 128;                 // tile columns (UMMA N)
+constexpr int TT_IMG_N = 128;             // rows of a B tile image (x)
 constexpr int TT_K = 32;                  // K per tile: one 128-byte swizzle row of TF32
 constexpr int TT_BYTES = TT_M * TT_K * 4; // 16 KB tile image
 constexpr int TT_FLOATS = TT_BYTES / 4;
-constexpr int TT_NS = 3;                  // pipeline stages, 4 tiles each
-constexpr int TT_THREADS = 128;
-constexpr size_t TT_SMEM = (size_t)TT_NS * 4 * TT_BYTES + 1024;  // + alignment slack
-constexpr uint32_t TT_TMEM_COLS = 128;    // FP32 accumulator 128 lanes x 128 columns
 
-// instruction descriptor, kind::tf32: D F32 (bits 4-5 = 1), A and B TF32
-// (bits 7-9, 10-12 = 2), both K-major (bits 15, 16 = 0), N >> 3 at bit 17,
-// M >> 4 at bit 24
-constexpr uint32_t kIdescTF32 =
-    (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TT_N >> 3) << 17) | ((uint32_t)(TT_M >> 4) << 24);
+// instruction descriptor, kind::tf32 (WS_IDESC below): D F32 (bits 4-5 =
+// 1), A and B TF32 (bits 7-9, 10-12 = 2), both K-major (bits 15, 16 = 0),
+// N >> 3 at bit 17, M >> 4 at bit 24
 
 // byte offset of element (row r, k-column c) in a 128 x 32 TF32 tile image
 __host__ __device__ __forceinline__ unsigned tile_off(int r, int c) {
@@ -152,9 +141,9 @@ __global__ void __launch_bounds__(256)
   __shared__ __align__(16) float sl[TT_FLOATS];
   const int nt = blockIdx.x, kt = blockIdx.y, k = blockIdx.z;
   const double* G = arrs.p[k];
-  for (int i = threadIdx.x; i < TT_K * TT_N; i += 256) {
-    const int zz = i / TT_N, xx = i - zz * TT_N;
-    const int x = nt * TT_N + xx, z = kt * TT_K + zz;
+  for (int i = threadIdx.x; i < TT_K * TT_IMG_N; i += 256) {
+    const int zz = i / TT_IMG_N, xx = i - zz * TT_IMG_N;
+    const int x = nt * TT_IMG_N + xx, z = kt * TT_K + zz;
     const double g = (x < nx) ? G[(size_t)z * nx + x] : 0.0;
     float hi, lo;
     split_f64(g, hi, lo);
@@ -173,51 +162,86 @@ __global__ void __launch_bounds__(256)
 }
 
 // ---- the GEMM -----------------------------------------------------------
+//
+// Persistent and warp-specialised: one CTA per SM walks a list of 128x128
+// output tiles.  Warp 0 (one lane) streams operand tiles through a 3-stage
+// shared-memory ring; warp 1 owns tensor memory and (one lane) issues the
+// MMAs into one of two accumulators; warps 2-5 drain the other accumulator
+// (tcgen05.ld; warp w reads TMEM lanes 32*(w%4)..+31), so the epilogue of a
+// tile overlaps the main loop of the next.
+//
+//   EPI_COEF  (GEMM 1)  D[j, x] = sum_z Wt[j, z] G[z, x]; tiles (array, x-tile,
+//                       j-tile), j fastest; epilogue: C = inv2 * D, split,
+//                       into the C^T image (a warp covers one 128-byte row).
+//   EPI_APPLY (GEMM 2)  D[x, z] = sum_j C^T[x, j] W[z, j] (the transposed
+//                       product, so a thread owns one x); tiles (array, x-tile,
+//                       z-tile), z fastest; epilogue: G[z, x] -= D, 32
+//                       coalesced FP64 rows per chunk straight from registers.
 
 struct Tf32GemmArgs {
-  const float* a_hi;  // A tile images [mt][KT]
+  const float* a_hi;  // A tile images
   const float* a_lo;
-  const float* b_hi;  // B tile images [array][nt][KT]
+  const float* b_hi;  // B tile images
   const float* b_lo;
   int KT;             // K tiles
-  int NT;             // N tiles per array
-  // EPI_COEF: C^T image out, [array][nt][KT2] tiles (rows x, k = j)
+  int NT;             // x tile images (128 rows of x) per array
+  int MT;             // tiles of the other output dimension (j or z)
+  int narr;
+  // EPI_COEF: C^T image out, [array][x-tile][KT2] tiles (rows x, k = j)
   float* c_hi;
   float* c_lo;
   int KT2;
   float scale;
-  // EPI_APPLY: G_k[z, x] -= D[z, x]
+  // EPI_APPLY: G_k[z, x] -= D[x, z]
   ArrayList arrs;
   int nx;
   unsigned* err;
 };
 
 constexpr int EPI_COEF = 0, EPI_APPLY = 1;
+constexpr int WS_NS = 3;                         // operand ring stages
+constexpr int WS_STAGE = 4 * TT_BYTES;           // A hi, A lo, B hi, B lo
+constexpr int WS_THREADS = 192;                  // producer, MMA, 4 epilogue warps
+constexpr uint32_t WS_TMEM_COLS = 256;           // two 128-column FP32 accumulators
+constexpr size_t WS_SMEM = (size_t)WS_NS * WS_STAGE + 1024;
+constexpr uint32_t WS_IDESC =
+    (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(128 >> 3) << 17) | ((uint32_t)(TT_M >> 4) << 24);
 
 template <int EPI>
-__global__ void __launch_bounds__(TT_THREADS, 1) tf32x3_gemm_kernel(const __grid_constant__ Tf32GemmArgs g) {
+__device__ __forceinline__ void ws_tile(const Tf32GemmArgs& g, int t, int& k, int& xt, int& ot) {
+  ot = t % g.MT;              // j-tile (COEF) or z-tile (APPLY), fastest
+  xt = (t / g.MT) % g.NT;     // x tile image
+  k = t / (g.MT * g.NT);      // array
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(WS_THREADS, 1) tf32x3_gemm_ws(const __grid_constant__ Tf32GemmArgs g) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char* const smem =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
-  __shared__ __align__(8) uint64_t full[TT_NS];
-  __shared__ __align__(8) uint64_t empty[TT_NS];
-  __shared__ __align__(8) uint64_t done;
+  __shared__ __align__(8) uint64_t full[WS_NS];
+  __shared__ __align__(8) uint64_t empty[WS_NS];
+  __shared__ __align__(8) uint64_t acc_full[2];
+  __shared__ __align__(8) uint64_t acc_empty[2];
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int nt = blockIdx.x, mt = blockIdx.y, k = blockIdx.z;
   const int KT = g.KT;
+  const int ntiles = g.narr * g.NT * g.MT;
 
   if (tid == 0) {
-    for (int s = 0; s < TT_NS; ++s) {
+    for (int s = 0; s < WS_NS; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(&done, 1);
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&acc_full[a], 1);
+      mbar_init(&acc_empty[a], 4);  // one arrival per epilogue warp
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) {
+  if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
-                 "r"(TT_TMEM_COLS));
+                 "r"(WS_TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   tc_fence_before();
@@ -225,114 +249,135 @@ __global__ void __launch_bounds__(TT_THREADS, 1) tf32x3_gemm_kernel(const __grid
   tc_fence_after();
   const uint32_t tmem = tmem_base;
 
-  const float* const A_hi = g.a_hi + (size_t)mt * KT * TT_FLOATS;
-  const float* const A_lo = g.a_lo + (size_t)mt * KT * TT_FLOATS;
-  const size_t bt = ((size_t)k * g.NT + nt) * KT * TT_FLOATS;
-  const float* const B_hi = g.b_hi + bt;
-  const float* const B_lo = g.b_lo + bt;
-
-  if (warp == 0 && lane == 0) {
-    // producer: four 16 KB tile copies per stage
-    for (int kt = 0; kt < KT; ++kt) {
-      const int s = kt % TT_NS, u = kt / TT_NS;
-      if (u > 0) mbar_wait(&empty[s], (unsigned)((u - 1) & 1), g.err);
-      unsigned char* const st = smem + (size_t)s * 4 * TT_BYTES;
-      mbar_expect_tx(&full[s], 4u * TT_BYTES);
-      const size_t o = (size_t)kt * TT_FLOATS;
-      bulk_g2s(st, A_hi + o, TT_BYTES, &full[s]);
-      bulk_g2s(st + TT_BYTES, A_lo + o, TT_BYTES, &full[s]);
-      bulk_g2s(st + 2 * TT_BYTES, B_hi + o, TT_BYTES, &full[s]);
-      bulk_g2s(st + 3 * TT_BYTES, B_lo + o, TT_BYTES, &full[s]);
+  if (warp == 0) {
+    if (lane == 0) {
+      // producer: the operand tiles of every tile of this CTA, in order
+      int q = 0;  // k-tiles issued so far
+      for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        int k, xt, ot;
+        ws_tile<EPI>(g, t, k, xt, ot);
+        size_t a_off, b_off;
+        if (EPI == EPI_COEF) {
+          a_off = (size_t)ot * KT * TT_FLOATS;                           // Wt image [j-tile]
+          b_off = ((size_t)k * g.NT + xt) * KT * TT_FLOATS;              // G image [array][x-tile]
+        } else {
+          a_off = ((size_t)k * g.NT + xt) * KT * TT_FLOATS;              // C^T image [array][x-tile]
+          b_off = (size_t)ot * KT * TT_FLOATS;                           // W image [z-tile]
+        }
+        for (int kt = 0; kt < KT; ++kt, ++q) {
+          const int s = q % WS_NS, u = q / WS_NS;
+          if (u > 0) mbar_wait(&empty[s], (unsigned)((u - 1) & 1), g.err);
+          unsigned char* const st = smem + (size_t)s * WS_STAGE;
+          mbar_expect_tx(&full[s], (unsigned)WS_STAGE);
+          const size_t o = (size_t)kt * TT_FLOATS;
+          bulk_g2s(st, g.a_hi + a_off + o, TT_BYTES, &full[s]);
+          bulk_g2s(st + TT_BYTES, g.a_lo + a_off + o, TT_BYTES, &full[s]);
+          bulk_g2s(st + 2 * TT_BYTES, g.b_hi + b_off + o, TT_BYTES, &full[s]);
+          bulk_g2s(st + 3 * TT_BYTES, g.b_lo + b_off + o, TT_BYTES, &full[s]);
+        }
+      }
     }
-  } else if (warp == 1 && lane == 0) {
-    // MMA issuer: per stage and K step of 8, lo*hi + hi*lo + hi*hi
-    for (int kt = 0; kt < KT; ++kt) {
-      const int s = kt % TT_NS, u = kt / TT_NS;
-      mbar_wait(&full[s], (unsigned)(u & 1), g.err);
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // MMA issuer: tile i accumulates into accumulator i % 2 once the
+      // epilogue has drained that accumulator's previous tile
+      int q = 0, i = 0;
+      for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+        const int a = i & 1;
+        if (i >= 2) mbar_wait(&acc_empty[a], (unsigned)(((i >> 1) - 1) & 1), g.err);
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(a * 128);
+        for (int kt = 0; kt < KT; ++kt, ++q) {
+          const int s = q % WS_NS, u = q / WS_NS;
+          mbar_wait(&full[s], (unsigned)(u & 1), g.err);
+          tc_fence_after();
+          const uint32_t st = smem_u32(smem + (size_t)s * WS_STAGE);
+#pragma unroll
+          for (int kk = 0; kk < TT_K / 8; ++kk) {
+            const uint32_t off = (uint32_t)kk * 32u;  // 8 TF32 = 32 bytes along the swizzled row
+            const uint64_t ah = sw128_desc(st + off), al = sw128_desc(st + TT_BYTES + off);
+            const uint64_t bh = sw128_desc(st + 2 * TT_BYTES + off), bl = sw128_desc(st + 3 * TT_BYTES + off);
+            umma_tf32(d, al, bh, WS_IDESC, (kt | kk) != 0 ? 1u : 0u);
+            umma_tf32(d, ah, bl, WS_IDESC, 1u);
+            umma_tf32(d, ah, bh, WS_IDESC, 1u);
+          }
+          umma_commit(&empty[s]);  // stage s free once these MMAs have read it
+        }
+        umma_commit(&acc_full[a]);  // accumulator a holds tile i
+      }
+    }
+  } else {
+    // epilogue warps 2..5: TMEM lane quadrant w % 4, tile row = 32*(w%4) + lane
+    const int quad = warp & 3;
+    const int r = 32 * quad + lane;
+    int i = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+      int k, xt, ot;
+      ws_tile<EPI>(g, t, k, xt, ot);
+      const int a = i & 1;
+      mbar_wait(&acc_full[a], (unsigned)((i >> 1) & 1), g.err);
+      __syncwarp();
       tc_fence_after();
-      const uint32_t st = smem_u32(smem + (size_t)s * 4 * TT_BYTES);
-#pragma unroll
-      for (int kk = 0; kk < TT_K / 8; ++kk) {
-        const uint32_t off = (uint32_t)kk * 32u;  // 8 TF32 = 32 bytes along the swizzled row
-        const uint64_t ah = sw128_desc(st + off), al = sw128_desc(st + TT_BYTES + off);
-        const uint64_t bh = sw128_desc(st + 2 * TT_BYTES + off), bl = sw128_desc(st + 3 * TT_BYTES + off);
-        umma_tf32(tmem, al, bh, kIdescTF32, (kt | kk) != 0 ? 1u : 0u);
-        umma_tf32(tmem, ah, bl, kIdescTF32, 1u);
-        umma_tf32(tmem, ah, bh, kIdescTF32, 1u);
-      }
-      umma_commit(&empty[s]);  // stage s free once these MMAs have read it
-    }
-    umma_commit(&done);
-  }
-  __syncwarp();
-
-  // epilogue: warp w reads TMEM lanes 32w..32w+31 = tile rows
-  mbar_wait(&done, 0u, g.err);
-  __syncwarp();
-  tc_fence_after();
-  const int row = mt * TT_M + 32 * warp + lane;
-  // EPI_APPLY stages the tile in the (now idle) operand buffers as
-  // [128][129] floats (row padding: conflict-free both ways)
-  float* const dtile = reinterpret_cast<float*>(smem);
+      const uint32_t src = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(a * 128);
 #pragma unroll 1
-  for (int cc = 0; cc < TT_N; cc += 32) {
-    uint32_t v[32];
-    tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)cc, v);
-    if (EPI == EPI_COEF) {
-      // row = j; columns x = nt*128 + cc + i -> C^T image tile (nt, j/32),
-      // tile row cc + i, k-column j % 32 = lane: one 128-byte row per warp
-      const size_t t = (((size_t)k * g.NT + nt) * g.KT2 + (row >> 5)) * TT_FLOATS;
+      for (int cc = 0; cc < 128; cc += 32) {
+        uint32_t v[32];
+        tmem_ld32(src + (uint32_t)cc, v);
+        if (EPI == EPI_COEF) {
+          // row j = ot*128 + r; columns x = xt*128 + cc + i -> C^T image tile
+          // (xt, j/32), tile row cc + i, k-column j % 32 = lane
+          const int j = ot * TT_M + r;
+          const size_t tb = (((size_t)k * g.NT + xt) * g.KT2 + (j >> 5)) * TT_FLOATS;
 #pragma unroll
-      for (int i = 0; i < 32; ++i) {
-        float hi, lo;
-        split_f32(__uint_as_float(v[i]) * g.scale, hi, lo);
-        const unsigned o = tile_off(cc + i, lane) >> 2;
-        g.c_hi[t + o] = hi;
-        g.c_lo[t + o] = lo;
+          for (int c = 0; c < 32; ++c) {
+            float hi, lo;
+            split_f32(__uint_as_float(v[c]) * g.scale, hi, lo);
+            const unsigned o = tile_off(cc + c, lane) >> 2;
+            g.c_hi[tb + o] = hi;
+            g.c_lo[tb + o] = lo;
+          }
+        } else {
+          // row x = xt*128 + r; columns z = ot*128 + cc + c: G_k[z, x] -= D
+          const int x = xt * TT_IMG_N + r;
+          if (x < g.nx) {
+            double* const G = g.arrs.p[k] + (size_t)(ot * TT_M + cc) * g.nx + x;
+            const size_t ld = (size_t)g.nx;
+            double gv[32];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) gv[c] = G[(size_t)c * ld];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) G[(size_t)c * ld] = gv[c] - (double)__uint_as_float(v[c]);
+          }
+        }
       }
-    } else {
-      const int r = 32 * warp + lane;
-#pragma unroll
-      for (int i = 0; i < 32; ++i) dtile[r * (TT_N + 1) + cc + i] = __uint_as_float(v[i]);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) {
+        unsigned aa = smem_u32(&acc_empty[a]);
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(aa) : "memory");
+      }
     }
   }
+  __syncwarp();
   tc_fence_before();
   __syncthreads();
-  if (EPI == EPI_APPLY) {
-    // G_k[z, x] -= D[z, x]: one tile row at a time, thread = column (coalesced)
-    // (16 rows loaded before any is stored, so the loads overlap)
-    const int x = nt * TT_N + tid;
-    if (x < g.nx) {
-      double* const G = g.arrs.p[k] + (size_t)mt * TT_M * g.nx + x;
-      const size_t ld = (size_t)g.nx;
-#pragma unroll 1
-      for (int r0 = 0; r0 < TT_M; r0 += 16) {
-        double gv[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i) gv[i] = G[(size_t)(r0 + i) * ld];
-#pragma unroll
-        for (int i = 0; i < 16; ++i) G[(size_t)(r0 + i) * ld] = gv[i] - (double)dtile[(r0 + i) * (TT_N + 1) + tid];
-      }
-    }
-  }
-  if (warp == 0) {
+  if (warp == 1) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TT_TMEM_COLS));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(WS_TMEM_COLS));
   }
 }
 
 }  // namespace
 
-int tf32_ntiles(int nx) { return (nx + TT_N - 1) / TT_N; }
+int tf32_ntiles(int nx) { return (nx + TT_IMG_N - 1) / TT_IMG_N; }
 int tf32_jpad(int J) { return ((J + TT_M - 1) / TT_M) * TT_M; }
 size_t tf32_tile_floats() { return TT_FLOATS; }
 
 cudaError_t prepare_tf32() {
-  cudaError_t e = cudaFuncSetAttribute(tf32x3_gemm_kernel<EPI_COEF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)TT_SMEM);
+  cudaError_t e =
+      cudaFuncSetAttribute(tf32x3_gemm_ws<EPI_COEF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WS_SMEM);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(tf32x3_gemm_kernel<EPI_APPLY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)TT_SMEM);
+  return cudaFuncSetAttribute(tf32x3_gemm_ws<EPI_APPLY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WS_SMEM);
 }
 
 cudaError_t launch_tf32_w_images(const double* W, int ldw, int J, int nz, const Tf32BandImages& b, cudaStream_t s) {
@@ -349,13 +394,18 @@ cudaError_t launch_band_tf32(const ArrayList& arrs, int narr, const Tf32BandImag
   g_image_kernel<<<dim3(NT, KT1, narr), 256, 0, s>>>(arrs, nx, NT, KT1, w.gh, w.gl);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   Tf32GemmArgs g1{};
-  g1.a_hi = b.a1h;
+  g1.a_hi = b.a1h;  // Wt image [j-tile][KT1]
   g1.a_lo = b.a1l;
-  g1.b_hi = w.gh;
+  g1.b_hi = w.gh;   // G image [array][x-tile][KT1]
   g1.b_lo = w.gl;
   g1.KT = KT1;
   g1.NT = NT;
+  g1.MT = MT1;
+  g1.narr = narr;
   g1.c_hi = w.ch;
   g1.c_lo = w.cl;
   g1.KT2 = KT2;
@@ -363,16 +413,19 @@ cudaError_t launch_band_tf32(const ArrayList& arrs, int narr, const Tf32BandImag
   g1.arrs = arrs;
   g1.nx = nx;
   g1.err = err;
-  tf32x3_gemm_kernel<EPI_COEF><<<dim3(NT, MT1, narr), TT_THREADS, TT_SMEM, s>>>(g1);
+  const int t1 = narr * NT * MT1;
+  tf32x3_gemm_ws<EPI_COEF><<<std::min(t1, sms), WS_THREADS, WS_SMEM, s>>>(g1);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   Tf32GemmArgs g2 = g1;
-  g2.a_hi = b.a2h;
-  g2.a_lo = b.a2l;
-  g2.b_hi = w.ch;
-  g2.b_lo = w.cl;
+  g2.a_hi = w.ch;   // C^T image [array][x-tile][KT2]
+  g2.a_lo = w.cl;
+  g2.b_hi = b.a2h;  // W image [z-tile][KT2]
+  g2.b_lo = b.a2l;
   g2.KT = KT2;
-  tf32x3_gemm_kernel<EPI_APPLY><<<dim3(NT, MT2, narr), TT_THREADS, TT_SMEM, s>>>(g2);
+  g2.MT = MT2;
+  const int t2 = narr * NT * MT2;
+  tf32x3_gemm_ws<EPI_APPLY><<<std::min(t2, sms), WS_THREADS, WS_SMEM, s>>>(g2);
   return cudaGetLastError();
 }
 
