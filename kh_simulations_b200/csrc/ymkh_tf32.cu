@@ -132,8 +132,10 @@ __global__ void w_image_kernel(const double* __restrict__ W, int ldw, int J, int
 }
 
 // G_k[z, x] (FP64) -> B image of GEMM 1, tile (nt, kt) of array k: rows x,
-// k = z.  Coalesced reads along x; the swizzled tile is assembled in shared
-// memory and written out linearly.
+// k = z.  Thread (x, z-quad): four loads along z (each coalesced across the
+// warp's consecutive x), split, and one 16-byte store per hi/lo chunk into
+// the swizzled tile (the 8 rows of a wavefront hit 8 different chunks:
+// conflict-free); the tile is then written out linearly.
 __global__ void __launch_bounds__(256)
     g_image_kernel(const __grid_constant__ ArrayList arrs, int nx, int NT, int KT, float* __restrict__ gh,
                    float* __restrict__ gl) {
@@ -141,15 +143,23 @@ __global__ void __launch_bounds__(256)
   __shared__ __align__(16) float sl[TT_FLOATS];
   const int nt = blockIdx.x, kt = blockIdx.y, k = blockIdx.z;
   const double* G = arrs.p[k];
-  for (int i = threadIdx.x; i < TT_K * TT_IMG_N; i += 256) {
-    const int zz = i / TT_IMG_N, xx = i - zz * TT_IMG_N;
-    const int x = nt * TT_IMG_N + xx, z = kt * TT_K + zz;
-    const double g = (x < nx) ? G[(size_t)z * nx + x] : 0.0;
-    float hi, lo;
-    split_f64(g, hi, lo);
-    const unsigned o = tile_off(xx, zz) >> 2;
-    sh[o] = hi;
-    sl[o] = lo;
+  const int xx = threadIdx.x % TT_IMG_N, qh = threadIdx.x / TT_IMG_N;  // 2 halves of the 8 z-quads
+  const int x = nt * TT_IMG_N + xx;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int q = qh * 4 + j;  // 16-byte chunk (4 consecutive z) of the tile row
+    const int z = kt * TT_K + 4 * q;
+    double g[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) g[c] = (x < nx) ? G[(size_t)(z + c) * nx + x] : 0.0;
+    float4 h, l;
+    split_f64(g[0], h.x, l.x);
+    split_f64(g[1], h.y, l.y);
+    split_f64(g[2], h.z, l.z);
+    split_f64(g[3], h.w, l.w);
+    const unsigned o = tile_off(xx, 4 * q) >> 2;
+    *reinterpret_cast<float4*>(sh + o) = h;
+    *reinterpret_cast<float4*>(sl + o) = l;
   }
   __syncthreads();
   const size_t t = (((size_t)k * NT + nt) * KT + kt) * TT_FLOATS;
