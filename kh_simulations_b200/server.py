@@ -31,13 +31,23 @@ BYTES_PER_CELL_STATE = 2 * 24 * 8  # two 24-array FP64 buffers
 
 def footprint(cfg: RunConfig) -> int:
     """Device bytes a run holds while resident: both state buffers, the
-    band-filter twiddles and coefficients, diagnostics (include/ymkh.h)."""
+    band-filter twiddles and coefficient scratch of its filter engine,
+    diagnostics (the allocations of include/ymkh.h's context)."""
     d = derive(cfg)
     cells = d.nx * d.nz
     fp = BYTES_PER_CELL_STATE * cells
     if d.bands:
-        maxj = max(2 * (hi - lo + 1) for lo, hi in d.bands)
-        fp += 21 * maxj * d.nx * 8 + sum(2 * (hi - lo + 1) * d.nz * 8 for lo, hi in d.bands)
+        js = [2 * (hi - lo + 1) for lo, hi in d.bands]
+        fp += sum(j * d.nz * 8 for j in js)  # FP64 twiddle matrices
+        if cfg.filter_engine == "tf32x3":
+            # TF32 hi/lo tile images: twiddles (both orientations) per band,
+            # G and C^T of the 21 filtered arrays (x padded to 128, j to 128)
+            xpad = -(-d.nx // 128) * 128
+            jpad = [-(-j // 128) * 128 for j in js]
+            fp += sum(4 * jp * d.nz * 4 for jp in jpad)
+            fp += 2 * 21 * xpad * d.nz * 4 + 2 * 21 * xpad * max(jpad) * 4
+        else:
+            fp += 21 * max(js) * d.nx * 8  # FP64 coefficients
     fp += 64 * 1024 + 16 * d.nx
     return fp
 

@@ -80,3 +80,18 @@ def test_defaults_and_extension_bands():
     assert d.bands == [(3, 4), (9, 9), (86, 128)]
     d = derive(loads("run_mode = 0\n"))
     assert d.periodic_x == 0 and d.freeze_az1 == 0 and d.energy_thresh == 5.0
+
+
+def test_filter_engine_key():
+    """Extension key `filter_engine` selects the band filter engine of the
+    C ABI (YMKH_FILTER_DFT = 0, YMKH_FILTER_TF32X3 = 1); other values are
+    rejected when the step parameters are formed."""
+    import pytest
+
+    from kh_simulations_b200.config import ConfigError, loads, step_params
+
+    base = "nz_override = 128\nnx_override = 256\nkz_keep_max = 42\n"
+    assert step_params(loads(base)).filter_engine == 0
+    assert step_params(loads(base + "filter_engine = tf32x3\n")).filter_engine == 1
+    with pytest.raises(ConfigError):
+        step_params(loads(base + "filter_engine = fp16\n"))

@@ -20,6 +20,16 @@ def test_footprint_counts_two_buffers_and_filter_scratch():
     assert footprint(cfg(64, 128, "kz_keep_max = 21\n")) > base
 
 
+def test_footprint_of_the_tensor_core_filter():
+    """The TF32 engine holds hi/lo tile images of the 21 filtered arrays
+    (G: 8 bytes per array cell, x padded to 128) and of the coefficients."""
+    fp64 = footprint(cfg(1024, 2048, "kz_keep_max = 341\n"))
+    tf32 = footprint(cfg(1024, 2048, "kz_keep_max = 341\nfilter_engine = tf32x3\n"))
+    g_images = 2 * 21 * 2048 * 1024 * 4
+    assert tf32 - fp64 > g_images - 21 * 342 * 2048 * 8
+    assert tf32 > 2 * 24 * 8 * 1024 * 2048 + g_images
+
+
 def test_fifo_admission_respects_budget_and_rejects_oversize():
     small, big = cfg(32, 64), cfg(256, 512)
     budget = 3 * footprint(small)
