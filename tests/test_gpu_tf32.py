@@ -73,3 +73,39 @@ def test_tf32x3_rejects_nz_not_multiple_of_128(cuda):
 
     with pytest.raises(YMKHError, match="multiple of 128"):
         KHRun(loads(BASE + "nz_override = 96\nnx_override = 128\nkz_keep_max = 32\nfilter_engine = tf32x3\n"))
+
+
+def test_tf32x3_run_in_a_batch_equals_alone(cuda):
+    """The tensor-core filter is deterministic (every output element is one
+    CTA's fixed MMA sequence): a TF32 run stepped inside a batch beside an
+    FP64-filter run is bit-identical to the same runs stepped alone."""
+    from kh_simulations_b200.batch import KHBatch
+    from kh_simulations_b200.config import loads
+    from kh_simulations_b200.run import KHRun
+
+    texts = [BASE + "nz_override = 128\nnx_override = 256\nkz_keep_max = 42\nfilter_engine = tf32x3\n",
+             BASE + "nz_override = 64\nnx_override = 128\nkz_keep_max = 21\n",
+             BASE + "nz_override = 256\nnx_override = 200\nkz_suppress_max = 3\nkz_suppress_hi = 20\n"
+             "suppress_kz0 = 1\nfilter_engine = tf32x3\n"]
+    alone = []
+    for t in texts:
+        r = KHRun(loads(t))
+        r.init()
+        r.add_noise(sigma=1e-4, seed=2)
+        s0 = r.state_numpy()
+        r.step(6)
+        alone.append((s0, r.state_numpy()))
+        r.close()
+    runs = []
+    batch = KHBatch()
+    for t, (s0, _) in zip(texts, alone):
+        r = KHRun(loads(t))
+        r.set_state(s0)
+        batch.add(r)
+        runs.append(r)
+    batch.step(6)
+    for r, (_, s6) in zip(runs, alone):
+        assert np.array_equal(r.state_numpy(), s6)
+    batch.close()
+    for r in runs:
+        r.close()
