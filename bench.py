@@ -453,16 +453,18 @@ def served_rate(args, dev, seconds: float) -> dict:
     at 20 runs/s for `seconds` s (seed 3), cells log-uniform in
     [128*256, 2048*4096], steps uniform in [20, 200] (the full mix has
     2000..20000: scaled by 1/100 so both passes finish in seconds), 150 GB
-    admission budget.  Continuous batching (KHServer.serve) against the same
-    requests one by one through the plain step (serve_sequential); p50/p99
-    run latency from arrival to completion; per-request final energies of
-    the two passes are compared."""
+    admission budget, split-precision filtering on (modes above NZ/3
+    subtracted with the 3-pass TF32 tensor-core filter).  Continuous
+    batching (KHServer.serve) against the same requests one by one through
+    the plain step (serve_sequential); p50/p99 run latency from arrival to
+    completion; per-request final energies of the two passes are compared."""
     import math
 
     from kh_simulations_b200.server import KHServer, poisson_mix
 
     def mix():
-        return poisson_mix(3, 20.0, seconds, 128 * 256, 2048 * 4096, 20, 200, SWEEP_BASE)
+        return poisson_mix(3, 20.0, seconds, 128 * 256, 2048 * 4096, 20, 200, SWEEP_BASE, keep_third=True,
+                           filter_engine="tf32x3")
 
     srv = KHServer(150 << 30, device=dev, chunk=50)
     served = srv.serve(mix())
@@ -472,7 +474,8 @@ def served_rate(args, dev, seconds: float) -> dict:
               if math.isfinite(r.energy) and r.energy != 0), default=0.0)
     a, b = served.summary(), seq.summary()
     keys = ("requests", "completed", "halted", "makespan_s", "cell_steps_per_s", "p50_latency_s", "p99_latency_s")
-    return {"workload": f"Poisson 20/s for {seconds:g} s (seed 3), 128x256..2048x4096 cells, 20..200 steps, 150 GB budget",
+    return {"workload": f"Poisson 20/s for {seconds:g} s (seed 3), 128x256..2048x4096 cells, 20..200 steps, "
+                        "150 GB budget, keep |k| <= NZ/3 with the TF32 tensor-core filter",
             "served": {k: a[k] for k in keys}, "sequential": {k: b[k] for k in keys},
             "served_over_sequential": a["cell_steps_per_s"] / b["cell_steps_per_s"] if b["cell_steps_per_s"] else None,
             "max_rel_energy_diff": de, "unit": "cell-steps/s", "latency_clock": "host wall clock (arrival to completion)"}

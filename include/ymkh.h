@@ -61,7 +61,7 @@ enum {
                             (ymgpu2d/YM_Physics.cu:349-584) */
   YMKH_FILTER_TF32X3 = 1 /* the same two contractions on the tensor cores: operands split
                             into TF32 hi + lo, three passes, FP32 accumulation (a precision
-                            change confined to the subtracted band; NZ a multiple of 128).
+                            change confined to the subtracted band).
                             No reference counterpart. */
 };
 

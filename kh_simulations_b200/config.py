@@ -14,7 +14,7 @@ Extension keys (not in the reference; they never change the step itself):
   ``kz_bands = a-b,c-d`` explicit extra subtraction bands
   ``filter_engine = dft | tf32x3``  how the band filter runs: FP64 sums with
                         the reference's FP32 twiddles (default), or the
-                        tensor cores with 3-pass split TF32 (NZ % 128 == 0)
+                        tensor cores with 3-pass split TF32
 """
 from __future__ import annotations
 

@@ -139,8 +139,8 @@ void free_bands(ymkh_ctx* c) {
 
 // TF32 engine set-up: twiddle tile images per band and the shared scratch.
 int setup_tf32(ymkh_ctx* c) {
-  if (c->nz % 128 != 0) return set_err(YMKH_EINVAL, "the TF32X3 filter needs NZ a multiple of 128 (got %d)", c->nz);
   CK(prepare_tf32(), "TF32 GEMM shared-memory attribute");
+  const size_t zp = (size_t)tf32_zpad(c->nz);
   const size_t tf = tf32_tile_floats();
   const size_t nt = (size_t)tf32_ntiles(c->nx);
   int maxJp = 0;
@@ -149,12 +149,12 @@ int setup_tf32(ymkh_ctx* c) {
     t.J = c->J[b];
     t.Jp = tf32_jpad(c->J[b]);
     maxJp = std::max(maxJp, t.Jp);
-    const size_t n = (size_t)t.Jp * c->nz;  // floats per image
+    const size_t n = (size_t)t.Jp * zp;  // floats per image
     for (float** q : {&t.a1h, &t.a1l, &t.a2h, &t.a2l}) CK(cudaMalloc(q, n * sizeof(float)), "cudaMalloc TF32 twiddle images");
     CK(launch_tf32_w_images(c->W[b], c->J[b], c->J[b], c->nz, t, 0), "TF32 twiddle images");
     g_launches++;
   }
-  const size_t ng = 21 * nt * (size_t)(c->nz / 32) * tf, nc = 21 * nt * (size_t)(maxJp / 32) * tf;
+  const size_t ng = 21 * nt * (zp / 32) * tf, nc = 21 * nt * (size_t)(maxJp / 32) * tf;
   CK(cudaMalloc(&c->tfs.gh, ng * sizeof(float)), "cudaMalloc TF32 G images");
   CK(cudaMalloc(&c->tfs.gl, ng * sizeof(float)), "cudaMalloc TF32 G images");
   CK(cudaMalloc(&c->tfs.ch, nc * sizeof(float)), "cudaMalloc TF32 coefficient images");
@@ -166,8 +166,6 @@ int setup_params(ymkh_ctx* c, const ymkh_params* p) {
   if (p->dt_step <= 0 || p->dx <= 0 || p->dz <= 0) return set_err(YMKH_EINVAL, "dx, dz, dt_step must be > 0");
   if (p->filter_engine != YMKH_FILTER_DFT && p->filter_engine != YMKH_FILTER_TF32X3)
     return set_err(YMKH_EINVAL, "unknown filter_engine %d", p->filter_engine);
-  if (p->filter_engine == YMKH_FILTER_TF32X3 && c->nz % 128 != 0)
-    return set_err(YMKH_EINVAL, "the TF32X3 filter needs NZ a multiple of 128 (got %d)", c->nz);
   if (p->suppress_kz0 && (c->nz & (c->nz - 1)) != 0)
     return set_err(YMKH_EINVAL, "suppress_kz0 requires NZ a power of 2 (got %d)", c->nz);
   if (p->n_extra_bands < 0 || p->n_extra_bands > YMKH_MAX_EXTRA_BANDS)

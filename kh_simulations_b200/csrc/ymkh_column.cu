@@ -16,6 +16,8 @@
 
 #include "ymkh_common.cuh"
 
+#include <mutex>
+
 namespace ymkh {
 
 // ---------------------------------------------------------------- twiddles
@@ -146,14 +148,23 @@ cudaError_t launch_hyperdiff(const ArrayList& a12, int nx, int nz, double mu, cu
 }
 
 // Column kernels keep a block of whole columns in shared memory.
+// The dynamic shared-memory limit is a property of the kernel, shared by
+// every run in the process: it only ever grows (to the largest NZ seen), so
+// a run with a smaller NZ never lowers it under a larger resident run.
 cudaError_t prepare_column(int nz) {
+  static std::mutex mu;
+  static size_t granted[64];  // per device
   const size_t smem = (size_t)nz * (ZM_CX > HD_CX ? ZM_CX : HD_CX) * sizeof(double);
   if (smem > 200 * 1024) return cudaErrorInvalidValue;
-  if (smem > 48 * 1024) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(mu);
+  if (smem > 48 * 1024 && smem > granted[dev]) {
     cudaError_t e = cudaFuncSetAttribute(zmean_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(hyperdiff_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    granted[dev] = smem;
   }
   return cudaSuccess;
 }

@@ -135,16 +135,17 @@ cudaError_t launch_init(const State& st, const InitArgs& a, cudaStream_t s);
 // the twiddle matrix as TF32 hi/lo tile images for both contractions;
 // shared scratch: the G and C^T tile images of the filtered arrays.
 struct Tf32BandImages {
-  float *a1h, *a1l;  // rows j, k = z: [Jp/128][NZ/32] tiles
-  float *a2h, *a2l;  // rows z, k = j: [NZ/128][Jp/32] tiles
+  float *a1h, *a1l;  // rows j, k = z: [Jp/128][Zp/32] tiles (Zp = NZ padded to 128)
+  float *a2h, *a2l;  // rows z, k = j: [Zp/128][Jp/32] tiles
   int J, Jp;
 };
 struct Tf32Scratch {
-  float *gh, *gl;    // [narr][NT][NZ/32] tiles
+  float *gh, *gl;    // [narr][NT][Zp/32] tiles
   float *ch, *cl;    // [narr][NT][Jp/32] tiles
 };
 int tf32_ntiles(int nx);
 int tf32_jpad(int J);
+int tf32_zpad(int nz);
 size_t tf32_tile_floats();
 cudaError_t prepare_tf32();
 cudaError_t launch_tf32_w_images(const double* W, int ldw, int J, int nz, const Tf32BandImages& b, cudaStream_t s);

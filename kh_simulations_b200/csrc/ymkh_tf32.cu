@@ -24,7 +24,9 @@
 //   W images  (built once per band):  A1 [mt = j/128][kt = z/32]   A2 [mt = z/128][kt = j/32]
 //   G image   (per step, per array):   [array][nt = x/128][kt = z/32]      (B of GEMM 1)
 //   C^T image (GEMM 1's epilogue):     [array][nt = x/128][kt = j/32]      (B of GEMM 2)
-// Rows beyond J or NX are zero.  NZ must be a multiple of 128.
+// z is padded to a multiple of 128 (Zp) and j to a multiple of 128 (Jp)
+// in the images; rows and k-columns beyond NZ, J or NX are zero, and GEMM 2
+// writes only z < NZ.
 //
 // The GEMM kernel is persistent and warp-specialised (see tf32x3_gemm_ws):
 // a producer lane streams operand tiles through a 3-stage ring of "full" /
@@ -113,16 +115,18 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 // ---- split kernels ------------------------------------------------------
 
 // W[z * ldw + j] (FP64 holding the FP32 twiddles) -> A1 (rows j, k = z) and
-// A2 (rows z, k = j) tile images, hi and lo; j in [J, Jp) is zero.
-__global__ void w_image_kernel(const double* __restrict__ W, int ldw, int J, int Jp, int nz, float* __restrict__ a1h,
-                               float* __restrict__ a1l, float* __restrict__ a2h, float* __restrict__ a2l) {
+// A2 (rows z, k = j) tile images, hi and lo, over z < Zp and j < Jp; the
+// padding (z >= nz or j >= J) is zero.
+__global__ void w_image_kernel(const double* __restrict__ W, int ldw, int J, int Jp, int nz, int Zp,
+                               float* __restrict__ a1h, float* __restrict__ a1l, float* __restrict__ a2h,
+                               float* __restrict__ a2l) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int z = blockIdx.y;
-  if (j >= Jp || z >= nz) return;
-  const float w = (j < J) ? (float)W[(size_t)z * ldw + j] : 0.0f;
+  if (j >= Jp || z >= Zp) return;
+  const float w = (j < J && z < nz) ? (float)W[(size_t)z * ldw + j] : 0.0f;
   float hi, lo;
   split_f32(w, hi, lo);
-  const int kt1 = nz / TT_K, kt2 = Jp / TT_K;
+  const int kt1 = Zp / TT_K, kt2 = Jp / TT_K;
   const size_t t1 = ((size_t)(j / TT_M) * kt1 + z / TT_K) * TT_FLOATS + (tile_off(j % TT_M, z % TT_K) >> 2);
   const size_t t2 = ((size_t)(z / TT_M) * kt2 + j / TT_K) * TT_FLOATS + (tile_off(z % TT_M, j % TT_K) >> 2);
   a1h[t1] = hi;
@@ -137,7 +141,7 @@ __global__ void w_image_kernel(const double* __restrict__ W, int ldw, int J, int
 // the swizzled tile (the 8 rows of a wavefront hit 8 different chunks:
 // conflict-free); the tile is then written out linearly.
 __global__ void __launch_bounds__(256)
-    g_image_kernel(const __grid_constant__ ArrayList arrs, int nx, int NT, int KT, float* __restrict__ gh,
+    g_image_kernel(const __grid_constant__ ArrayList arrs, int nx, int nz, int NT, int KT, float* __restrict__ gh,
                    float* __restrict__ gl) {
   __shared__ __align__(16) float sh[TT_FLOATS];
   __shared__ __align__(16) float sl[TT_FLOATS];
@@ -151,7 +155,7 @@ __global__ void __launch_bounds__(256)
     const int z = kt * TT_K + 4 * q;
     double g[4];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) g[c] = (x < nx) ? G[(size_t)(z + c) * nx + x] : 0.0;
+    for (int c = 0; c < 4; ++c) g[c] = (x < nx && z + c < nz) ? G[(size_t)(z + c) * nx + x] : 0.0;
     float4 h, l;
     split_f64(g[0], h.x, l.x);
     split_f64(g[1], h.y, l.y);
@@ -205,6 +209,7 @@ struct Tf32GemmArgs {
   // EPI_APPLY: G_k[z, x] -= D[x, z]
   ArrayList arrs;
   int nx;
+  int nz;
   unsigned* err;
 };
 
@@ -348,15 +353,23 @@ __global__ void __launch_bounds__(WS_THREADS, 1) tf32x3_gemm_ws(const __grid_con
           }
         } else {
           // row x = xt*128 + r; columns z = ot*128 + cc + c: G_k[z, x] -= D
+          // (z < nz; the padded rows of a last partial z tile are skipped)
           const int x = xt * TT_IMG_N + r;
-          if (x < g.nx) {
-            double* const G = g.arrs.p[k] + (size_t)(ot * TT_M + cc) * g.nx + x;
+          const int z0 = ot * TT_M + cc;
+          if (x < g.nx && z0 < g.nz) {
+            double* const G = g.arrs.p[k] + (size_t)z0 * g.nx + x;
             const size_t ld = (size_t)g.nx;
-            double gv[32];
+            if (z0 + 32 <= g.nz) {
+              double gv[32];
 #pragma unroll
-            for (int c = 0; c < 32; ++c) gv[c] = G[(size_t)c * ld];
+              for (int c = 0; c < 32; ++c) gv[c] = G[(size_t)c * ld];
 #pragma unroll
-            for (int c = 0; c < 32; ++c) G[(size_t)c * ld] = gv[c] - (double)__uint_as_float(v[c]);
+              for (int c = 0; c < 32; ++c) G[(size_t)c * ld] = gv[c] - (double)__uint_as_float(v[c]);
+            } else {
+#pragma unroll
+              for (int c = 0; c < 32; ++c)
+                if (z0 + c < g.nz) G[(size_t)c * ld] = G[(size_t)c * ld] - (double)__uint_as_float(v[c]);
+            }
           }
         }
       }
@@ -381,6 +394,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) tf32x3_gemm_ws(const __grid_con
 
 int tf32_ntiles(int nx) { return (nx + TT_IMG_N - 1) / TT_IMG_N; }
 int tf32_jpad(int J) { return ((J + TT_M - 1) / TT_M) * TT_M; }
+int tf32_zpad(int nz) { return ((nz + TT_M - 1) / TT_M) * TT_M; }
 size_t tf32_tile_floats() { return TT_FLOATS; }
 
 cudaError_t prepare_tf32() {
@@ -391,17 +405,18 @@ cudaError_t prepare_tf32() {
 }
 
 cudaError_t launch_tf32_w_images(const double* W, int ldw, int J, int nz, const Tf32BandImages& b, cudaStream_t s) {
-  if (nz % TT_M != 0) return cudaErrorInvalidValue;
-  dim3 grid((b.Jp + 127) / 128, nz);
-  w_image_kernel<<<grid, 128, 0, s>>>(W, ldw, J, b.Jp, nz, b.a1h, b.a1l, b.a2h, b.a2l);
+  const int Zp = tf32_zpad(nz);
+  dim3 grid((b.Jp + 127) / 128, Zp);
+  w_image_kernel<<<grid, 128, 0, s>>>(W, ldw, J, b.Jp, nz, Zp, b.a1h, b.a1l, b.a2h, b.a2l);
   return cudaGetLastError();
 }
 
 cudaError_t launch_band_tf32(const ArrayList& arrs, int narr, const Tf32BandImages& b, const Tf32Scratch& w, int nx,
                              int nz, float inv2, unsigned* err, cudaStream_t s) {
-  if (nz % TT_M != 0 || narr < 1) return cudaErrorInvalidValue;
-  const int NT = tf32_ntiles(nx), KT1 = nz / TT_K, MT1 = b.Jp / TT_M, KT2 = b.Jp / TT_K, MT2 = nz / TT_M;
-  g_image_kernel<<<dim3(NT, KT1, narr), 256, 0, s>>>(arrs, nx, NT, KT1, w.gh, w.gl);
+  if (narr < 1) return cudaErrorInvalidValue;
+  const int Zp = tf32_zpad(nz);
+  const int NT = tf32_ntiles(nx), KT1 = Zp / TT_K, MT1 = b.Jp / TT_M, KT2 = b.Jp / TT_K, MT2 = Zp / TT_M;
+  g_image_kernel<<<dim3(NT, KT1, narr), 256, 0, s>>>(arrs, nx, nz, NT, KT1, w.gh, w.gl);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148;
@@ -422,6 +437,7 @@ cudaError_t launch_band_tf32(const ArrayList& arrs, int narr, const Tf32BandImag
   g1.scale = inv2;
   g1.arrs = arrs;
   g1.nx = nx;
+  g1.nz = nz;
   g1.err = err;
   const int t1 = narr * NT * MT1;
   tf32x3_gemm_ws<EPI_COEF><<<std::min(t1, sms), WS_THREADS, WS_SMEM, s>>>(g1);

@@ -41,11 +41,12 @@ def footprint(cfg: RunConfig) -> int:
         fp += sum(j * d.nz * 8 for j in js)  # FP64 twiddle matrices
         if cfg.filter_engine == "tf32x3":
             # TF32 hi/lo tile images: twiddles (both orientations) per band,
-            # G and C^T of the 21 filtered arrays (x padded to 128, j to 128)
+            # G and C^T of the 21 filtered arrays (x, z and j padded to 128)
             xpad = -(-d.nx // 128) * 128
+            zpad = -(-d.nz // 128) * 128
             jpad = [-(-j // 128) * 128 for j in js]
-            fp += sum(4 * jp * d.nz * 4 for jp in jpad)
-            fp += 2 * 21 * xpad * d.nz * 4 + 2 * 21 * xpad * max(jpad) * 4
+            fp += sum(4 * jp * zpad * 4 for jp in jpad)
+            fp += 2 * 21 * xpad * zpad * 4 + 2 * 21 * xpad * max(jpad) * 4
         else:
             fp += 21 * max(js) * d.nx * 8  # FP64 coefficients
     fp += 64 * 1024 + 16 * d.nx
@@ -253,13 +254,16 @@ class KHServer:
 
 
 def poisson_mix(seed: int, rate: float, duration: float, min_cells: int, max_cells: int, min_steps: int,
-                max_steps: int, base_ini: str, nz_multiple: int = 32) -> list:
+                max_steps: int, base_ini: str, nz_multiple: int = 32, keep_third: bool = False,
+                filter_engine: str = "dft") -> list:
     """Seeded request mix: Poisson arrivals at `rate` per second for
     `duration` seconds; cell counts log-uniform in [min_cells, max_cells]
     with NZ:NX = 1:2 (NZ rounded to a multiple of nz_multiple, a power of two
     when the run suppresses kz=0); V0 ~ U[0.02, 0.2], shear width
     ~ U[0.5, 2], kz in {0..3}, perturbation ~ U[0.05, 0.2]; kz = 0 suppressed
-    in every other request; steps uniform in [min_steps, max_steps]."""
+    in every other request; steps uniform in [min_steps, max_steps].  With
+    keep_third, every request filters modes above NZ/3 with the given
+    filter engine."""
     from .config import loads
 
     rng = np.random.default_rng(seed)
@@ -290,6 +294,8 @@ def poisson_mix(seed: int, rate: float, duration: float, min_cells: int, max_cel
         ini = (base_ini + f"k_mode = {kz}\nV0 = {v0:.6f}\neps_override = {eps:.6f}\nperturb_amp = {amp:.6f}\n"
                f"nz_override = {nz}\nnx_override = {nx}\ncourant_override = {courant:.6f}\n"
                f"suppress_kz0 = {1 if kz0 else 0}\n")
+        if keep_third:
+            ini += f"kz_keep_max = {nz // 3}\nfilter_engine = {filter_engine}\n"
         out.append(KHRequest(rid, loads(ini, f"req{rid}"), steps, t))
         rid += 1
     return out

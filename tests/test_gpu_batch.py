@@ -126,3 +126,20 @@ def test_autotune_runs_and_keeps_results(cuda, tmp_path, monkeypatch):
     assert np.array_equal(s_tuned.state_numpy(), _alone(MIX[2][0], 4))
     r.close()
     s_tuned.close()
+
+
+def test_runs_of_different_nz_in_one_process(cuda):
+    """The column kernels' shared-memory limit is per kernel, shared by all
+    runs of the process: creating a run with a smaller NZ must not lower it
+    under a resident run with a larger NZ (z-mean of NZ = 2048 needs 64 KB)."""
+    from kh_simulations_b200.run import KHRun
+
+    big = KHRun(_cfg("nz_override = 2048\nnx_override = 64\nsuppress_kz0 = 1\n"))
+    big.init()
+    small = KHRun(_cfg("nz_override = 1600\nnx_override = 64\n"))
+    small.init()
+    big.step(2)
+    small.step(2)
+    assert np.isfinite(big.state_numpy()).all() and np.isfinite(small.state_numpy()).all()
+    big.close()
+    small.close()
