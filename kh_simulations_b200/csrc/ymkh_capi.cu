@@ -231,9 +231,7 @@ void choose_launch_shape(ymkh_ctx* c) {
 
 // Row staging of the fused kernels when every bound array is 16-byte aligned
 // and x is periodic with nx even: TMA bulk row copies issued one per thread
-// across all warps.  Measured on B200 at 4096 x 8192: FCT 7.3 ms and Maxwell
-// 3.9 ms per step, against 9.0 / 4.5 ms with warp 0 issuing every copy and
-// 7.8 / 4.1 ms with 16-byte cp.async by every thread.
+// across all warps (RowLoad).
 constexpr int kAlignedRowLoad = LOAD_BULK_ALL;
 
 RunDesc make_desc(const ymkh_ctx* c, int start, int tb, int fct_item0, int mx_item0) {

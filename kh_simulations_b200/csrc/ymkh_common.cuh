@@ -73,11 +73,6 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
-// 16-byte form: both addresses 16-byte aligned; bypasses L1 (.cg).
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -212,10 +207,12 @@ __device__ __forceinline__ void bulk_row_periodic(double* dst, const double* row
 namespace ymkh {
 
 // How a fused kernel stages its rows (RunDesc::fct_bulk / mx_bulk).
+// Measured at 4096 x 8192 (FCT / Maxwell per step): TMA bulk rows issued
+// by warp 0 alone 9.0 / 4.5 ms, 16-byte cp.async by every thread 7.8 / 4.1
+// ms, bulk rows spread one per thread over all warps 7.3 / 3.9 ms (the form
+// kept).
 enum RowLoad : int {
   LOAD_ELEM = 0,    // per-element 8-byte cp.async through an x index table (walls, odd nx)
-  LOAD_BULK = 1,    // TMA bulk row copies issued by warp 0, mbarrier completion
-  LOAD_VEC16 = 2,   // 16-byte cp.async by every thread, periodic x with nx even
   LOAD_BULK_ALL = 3 // TMA bulk row copies, one per thread spread over all warps
 };
 

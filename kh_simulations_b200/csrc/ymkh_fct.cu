@@ -133,8 +133,7 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
     const int nx = p.nx, nz = p.nz;
     const bool warm = p.warm_T > 0.0;
     const bool wall = !p.periodic_x;
-    const int lmode = rd.fct_bulk;
-    const bool bulk = (lmode == LOAD_BULK || lmode == LOAD_BULK_ALL);  // mbarrier completion
+    const bool bulk = rd.fct_bulk == LOAD_BULK_ALL;  // TMA bulk rows on mbarriers (else per-element cp.async)
     const double dt = p.dt;
     const double dtdx = p.dt / p.dx;
     const double dtdz = p.dt / p.dz;
@@ -150,12 +149,12 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
     for (int i = tid; i < 2 * 2 * W; i += NT) wk[(size_t)(i / (2 * W)) * WB_SIZE * W + WB_SZ * W + i % (2 * W)] = 0.0;
     __syncthreads();
 
-    // LOAD_BULK_ALL: this thread's row copy for the item (array a of the
-    // stage, lane-major over the warps): source array, stage slot, which row
-    // (0: z, 1: z-1, 2: z+1) and the split at the periodic wrap
+    // bulk rows: this thread's row copy for the item (array a of the stage,
+    // lane-major over the warps): source array, stage slot, which row (0: z,
+    // 1: z-1, 2: z+1) and the split at the periodic wrap
     const double* cp_base = nullptr;
     int cp_dst = 0, cp_kind = 0, cp_x1 = 0, cp_len1 = W;
-    if (lmode == LOAD_BULK_ALL) {
+    if (bulk) {
       const int a = (tid & 31) * (NT / 32) + (tid >> 5);
       if (a < 33 + (warm ? 4 : 0)) {
         if (a < 12) {
@@ -185,38 +184,8 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
       const int zm = (zr == 0) ? nz - 1 : zr - 1;
       const int zp = (zr == nz - 1) ? 0 : zr + 1;
       const size_t ro = (size_t)zr * nx, rom = (size_t)zm * nx, rop = (size_t)zp * nx;
-      // Stage array a (0..narr): its source row and slot.
-      auto row_src = [&](int a, int& dsto) -> const double* {
-        if (a < 12) {
-          dsto = ST_FL + a;
-          return (a < 6 ? st.a[a] : st.b[a - 6]) + ro;
-        }
-        if (a < 33) {
-          const int kind = (a - 12) / 3, c = (a - 12) - kind * 3;  // EX, BY, BYM, EZ, EZM, AZ, AZM
-          const double* base = (kind == 0) ? st.f[EX1 + c]
-                               : (kind <= 2) ? st.f[BY1 + c]
-                               : (kind <= 4) ? st.f[EZ1 + c]
-                                             : st.f[AZ1 + c];
-          dsto = ST_EX + (a - 12);
-          return base + ((kind == 2 || kind == 4 || kind == 6) ? rom : ro);
-        }
-        const int w = a - 33;  // NZP A, NZP B, NZM A, NZM B
-        dsto = ST_NZP + w;
-        return ((w & 1) ? st.b[FN] : st.a[FN]) + ((w >> 1) ? rom : rop);
-      };
       const int narr = 33 + (warm ? 4 : 0);
-      const int xs = x0 - 4;
-      if (lmode == LOAD_BULK) {
-        if (tid < 32) {  // warp 0: lane 0 arms the stage, then each lane copies whole rows
-          if (tid == 0) mbar_expect_tx(&bars[s], (unsigned)(narr * W * 8));
-          __syncwarp();
-          for (int a = tid; a < narr; a += 32) {
-            int dsto;
-            const double* row = row_src(a, dsto);
-            bulk_row_periodic(sb + dsto * W, row, xs, W, nx, &bars[s]);
-          }
-        }
-      } else if (lmode == LOAD_BULK_ALL) {
+      if (bulk) {
         // one row copy per thread, spread over the warps (lane-major) so no
         // single warp serialises the issue; completions that land before
         // thread 0 arms the stage only drive its transaction count negative,
@@ -229,19 +198,6 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
           bulk_g2s(dst, cp_base + off + cp_x1, (unsigned)cp_len1 * 8u, &bars[s]);
           if (cp_len1 < W) bulk_g2s(dst + cp_len1, cp_base + off, (unsigned)(W - cp_len1) * 8u, &bars[s]);
         }
-      } else if (lmode == LOAD_VEC16) {
-        // 16-byte chunks (x even, nx even and >= W: a chunk never straddles
-        // the periodic wrap), spread over every thread
-        constexpr int NC = W / 2;
-        for (int i = tid; i < narr * NC; i += NT) {
-          const int a = i / NC, c = i - a * NC;
-          int dsto;
-          const double* row = row_src(a, dsto);
-          int x = xs + 2 * c;
-          x = x < 0 ? x + nx : (x >= nx ? x - nx : x);
-          cp_async16(sb + dsto * W + 2 * c, row + x);
-        }
-        cp_async_commit();
       } else {
         for (int i = tid; i < 12 * (W - 1); i += NT) {
           const int a = i / (W - 1), q = 1 + (i - a * (W - 1));

@@ -93,8 +93,7 @@ __global__ void __launch_bounds__(MX_NT, 4)
     __syncthreads();
     const int nx = p.nx, nz = p.nz;
     const bool wall = !p.periodic_x;
-    const int lmode = rd.mx_bulk;
-    const bool bulk = (lmode == LOAD_BULK || lmode == LOAD_BULK_ALL);  // mbarrier completion
+    const bool bulk = rd.mx_bulk == LOAD_BULK_ALL;  // TMA bulk rows on mbarriers (else per-element cp.async)
     const double dt = p.dt, c2 = p.c2, al = p.alpha, e0 = p.eps0;
     // c = eps_0 = 1 (ymgpu2d/main_ym.cu:69): 1*x and x/1 are exact, so the
     // products and quotients by them can be skipped without changing a bit
@@ -119,43 +118,17 @@ __global__ void __launch_bounds__(MX_NT, 4)
                : (kind == 2) ? fields_old.f[EX1 + c]
                              : fields_old.f[EZ1 + c];
       };
-      if (lmode == LOAD_BULK) {
-        if (tid < 32) {  // warp 0: lane 0 arms the stage, then each lane copies whole rows
-          if (tid == 0) mbar_expect_tx(&bars[s], (unsigned)(MS_SIZE * W * 8));
-          __syncwarp();
-          for (int a = tid; a < MS_SIZE; a += 32) bulk_row_periodic(sb + a * W, arr(a) + ro, x0 - 2, W, nx, &bars[s]);
-        }
-      } else if (lmode == LOAD_BULK_ALL) {
+      if (bulk) {
         // one row copy per thread, spread over the warps (lane-major); early
         // completions only drive the transaction count negative before
         // thread 0's arrival arms the phase
         if (tid == 0) mbar_expect_tx(&bars[s], (unsigned)(MS_SIZE * W * 8));
         const int a = (tid & 31) * (NT / 32) + (tid >> 5);
         if (a < MS_SIZE) bulk_row_periodic(sb + a * W, arr(a) + ro, x0 - 2, W, nx, &bars[s]);
-      } else if (lmode == LOAD_VEC16) {
-        // 16-byte chunks (x even, nx even and >= W: no chunk straddles the wrap)
-        constexpr int NC = W / 2;
-        for (int i = tid; i < MS_SIZE * NC; i += NT) {
-          const int a = i / NC, c = i - a * NC;
-          int x = x0 - 2 + 2 * c;
-          x = x < 0 ? x + nx : (x >= nx ? x - nx : x);
-          cp_async16(sb + a * W + 2 * c, arr(a) + ro + x);
-        }
-        cp_async_commit();
       } else {
         for (int i = tid; i < MS_SIZE * W; i += NT) {
           const int a = i / W, k = i - a * W;
-          const double* base;
-          if (a < 12)
-            base = (a < 6) ? fluid_new.a[a] : fluid_new.b[a - 6];
-          else {
-            const int kind = (a - 12) / 3, c = (a - 12) % 3;
-            base = (kind == 0) ? fields_old.f[BY1 + c]
-                   : (kind == 1) ? fields_old.f[AZ1 + c]
-                   : (kind == 2) ? fields_old.f[EX1 + c]
-                                 : fields_old.f[EZ1 + c];
-          }
-          cp_async8(sb + a * W + k, base + ro + xtab[k]);
+          cp_async8(sb + a * W + k, arr(a) + ro + xtab[k]);
         }
         cp_async_commit();
       }
