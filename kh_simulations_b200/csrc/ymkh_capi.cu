@@ -26,6 +26,8 @@
 #include <algorithm>
 #include "ymkh_common.cuh"
 
+#include <nvtx3/nvToolsExt.h>
+
 
 using namespace ymkh;
 
@@ -43,6 +45,13 @@ int set_err(int code, const char* fmt, ...) {
   va_end(ap);
   return code;
 }
+
+// NVTX range for the host timeline of a profiler (header-only NVTX 3: a
+// no-op unless a tool is attached).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
 
 #define CK(call, what)                                                                    \
   do {                                                                                    \
@@ -352,15 +361,22 @@ int step_once(ymkh_ctx* c, cudaStream_t s) {
   if (!c->desc_ok) { int rc = upload_desc(c); if (rc) return rc; }
   RunTable T{c->ddesc + c->cur, 1, c->fct_items, c->mx_items, c->derr, c->fx_items, c->fz_items};
   mark(c, ST_FCT, s);
-  if (c->fct_mode == YMKH_FCT_SPLIT) {
-    CK(launch_fct_split_table(T, c->fx_grid, c->fz_grid, s), "fct_x/fct_z kernels");
-    g_launches++;
-  } else {
-    CK(launch_fct_table(T, c->fct_tx, c->fct_grid, s), "fct_fused_kernel");
+  {
+    NvtxRange r("ymkh fct");
+    if (c->fct_mode == YMKH_FCT_SPLIT) {
+      CK(launch_fct_split_table(T, c->fx_grid, c->fz_grid, s), "fct_x/fct_z kernels");
+      g_launches++;
+    } else {
+      CK(launch_fct_table(T, c->fct_tx, c->fct_grid, s), "fct_fused_kernel");
+    }
   }
   mark(c, ST_MAXWELL, s);
-  CK(launch_maxwell_table(T, c->mx_grid, s), "maxwell_fused_kernel");
+  {
+    NvtxRange r("ymkh maxwell");
+    CK(launch_maxwell_table(T, c->mx_grid, s), "maxwell_fused_kernel");
+  }
   g_launches += 2;
+  NvtxRange r("ymkh column stages");
   int rc = post_stages(c, c->buf[1 - c->cur], s);
   if (rc) return rc;
   c->cur = 1 - c->cur;
@@ -577,6 +593,7 @@ int ymkh_step(ymkh_ctx* c, int nsteps, void* stream) {
   if (!c) return set_err(YMKH_EINVAL, "null context");
   if (!c->bound) return set_err(YMKH_ESTATE, "state not bound");
   if (nsteps < 0) return set_err(YMKH_EINVAL, "negative step count");
+  NvtxRange range("ymkh_step");
   cudaStream_t s = (cudaStream_t)stream;
   int done = 0;
   const bool graphs = s != nullptr && c->graph_steps >= 2 && (c->graph_steps % 2) == 0;
@@ -863,6 +880,7 @@ int ymkh_batch_set_graph_steps(ymkh_batch* b, int n) {
 int ymkh_batch_step(ymkh_batch* b, int nsteps, void* stream) {
   if (!b) return set_err(YMKH_EINVAL, "null batch");
   if (nsteps < 0) return set_err(YMKH_EINVAL, "negative step count");
+  NvtxRange range("ymkh_batch_step");
   cudaStream_t s = (cudaStream_t)stream;
   if (b->dirty) { int rc = batch_build(b); if (rc) return rc; }
   int done = 0;

@@ -53,6 +53,10 @@ class EnergyRecord:
     time: float
     energy: float
     ratio: float
+    mode_amp: float = math.nan  # k_mode amplitude of Az2 + i Az3 (when recorded)
+
+
+CHECKPOINT_VERSION = 1
 
 
 class KHRun:
@@ -162,10 +166,12 @@ class KHRun:
 
     # ------------------------------------------------------------------ loop
     def run(self, total_steps: int | None = None, energy_stride: int | None = None, csv: str | Path | None = None,
-            on_energy=None, stream=None) -> list:
+            on_energy=None, stream=None, mode_amp: bool = False) -> list:
         """The time loop of ymgpu2d/main_ym.cu:318-479 (without CSV snapshots):
         energy every ``energy_stride`` steps, halt on NaN/Inf or E/E0 above
-        the reference's threshold (:249, :467-474)."""
+        the reference's threshold (:249, :467-474).  With mode_amp, the
+        k_mode amplitude (offline in the reference,
+        analysis/remote_timeseries.py:62-77) is recorded at the same stride."""
         d = self.d
         total = d.total_steps if total_steps is None else total_steps
         stride = d.energy_stride if energy_stride is None else energy_stride
@@ -173,7 +179,8 @@ class KHRun:
         try:
             if self.E0 is None:
                 self.E0 = self.energy(stream)
-                self.history.append(EnergyRecord(0, 0.0, self.E0, 1.0))
+                amp0 = self.mode_amp(stream=stream)[0] if mode_amp else math.nan
+                self.history.append(EnergyRecord(0, 0.0, self.E0, 1.0, amp0))
                 if fh:
                     fh.write("step,time,E_total,E_ratio\n")
                     fh.write(f"0,0,{self.E0:.8e},1.0\n")
@@ -184,7 +191,8 @@ class KHRun:
                     E = self.energy(stream)
                     ratio = E / self.E0
                     t = self.step_count * d.dt
-                    rec = EnergyRecord(self.step_count, t, E, ratio)
+                    amp = self.mode_amp(stream=stream)[0] if mode_amp else math.nan
+                    rec = EnergyRecord(self.step_count, t, E, ratio, amp)
                     self.history.append(rec)
                     if fh:
                         fh.write(f"{self.step_count},{t:.8e},{E:.8e},{ratio:.8e}\n")
@@ -199,6 +207,37 @@ class KHRun:
             if fh:
                 fh.close()
         return self.history
+
+    # ------------------------------------------------------------ checkpoint
+    def save_checkpoint(self, path: str | Path) -> None:
+        """Raw FP64 state and loop position (.npz): the 24 arrays in
+        include/ymkh.h order, the step count, E0, the halt flag and the
+        energy history.  The reference has no checkpoint (its snapshots are
+        6-digit CSV, ymgpu2d/main_ym.cu:290-306); this one is exact, so a run
+        resumed from it continues bit for bit."""
+        h = self.history
+        np.savez(Path(path), version=CHECKPOINT_VERSION, state=self.state_numpy(), nx=self.d.nx, nz=self.d.nz,
+                 step_count=self.step_count, E0=np.nan if self.E0 is None else self.E0,
+                 halted=self.halted, halt_reason=self.halt_reason,
+                 hist=np.array([[r.step, r.time, r.energy, r.ratio, r.mode_amp] for r in h], dtype=np.float64)
+                 .reshape(len(h), 5))
+
+    def load_checkpoint(self, path: str | Path) -> None:
+        """Restore a checkpoint written by save_checkpoint for the same grid."""
+        with np.load(Path(path), allow_pickle=False) as z:
+            if int(z["version"]) != CHECKPOINT_VERSION:
+                raise ValueError(f"checkpoint version {int(z['version'])} != {CHECKPOINT_VERSION}")
+            if (int(z["nx"]), int(z["nz"])) != (self.d.nx, self.d.nz):
+                raise ValueError(f"checkpoint grid {int(z['nz'])}x{int(z['nx'])} != {self.d.nz}x{self.d.nx}")
+            self.set_state(z["state"])
+            self.step_count = int(z["step_count"])
+            e0 = float(z["E0"])
+            self.E0 = None if math.isnan(e0) else e0
+            self.halted = bool(z["halted"])
+            self.halt_reason = str(z["halt_reason"])
+            self.history = [EnergyRecord(int(r[0]), float(r[1]), float(r[2]), float(r[3]), float(r[4]))
+                            for r in z["hist"]]
+        torch.cuda.synchronize(self.device)
 
     def close(self) -> None:
         if getattr(self, "ctx", None):

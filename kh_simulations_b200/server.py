@@ -61,7 +61,8 @@ class KHRequest:
     arrival: float = 0.0           # seconds after the server starts
     admitted: float = math.nan
     finished: float = math.nan
-    status: str = "pending"        # pending | running | done | halted | rejected
+    status: str = "pending"        # pending | running | done | halted | rejected | cancelled
+    cancel_at: float = math.inf    # seconds after the server starts: withdrawn from then on
     energy: float = math.nan
     state: np.ndarray | None = None
 
@@ -94,6 +95,7 @@ class ServeReport:
         return {"mode": self.mode, "requests": len(self.requests), "completed": n_done,
                 "halted": sum(r.status == "halted" for r in self.requests),
                 "rejected": sum(r.status == "rejected" for r in self.requests),
+                "cancelled": sum(r.status == "cancelled" for r in self.requests),
                 "makespan_s": self.makespan, "cell_steps": self.cell_steps,
                 "cell_steps_per_s": self.cell_steps_per_s, "p50_latency_s": self.p50, "p99_latency_s": self.p99,
                 **self.extra}
@@ -175,6 +177,9 @@ class KHServer:
         first = pending[0].arrival if pending else 0.0
         while pending or active:
             now = self.clock() - t0
+            for req in [r for r in pending if r.cancel_at <= now]:  # withdrawn before admission
+                pending.remove(req)
+                req.status, req.finished = "cancelled", now
             for req, fp in self.admit_order(pending, now, used):
                 run = self._start_run(req)
                 req.admitted = self.clock() - t0
@@ -198,6 +203,8 @@ class KHServer:
                 status = None
                 if rem <= 0:
                     status = "done"
+                elif req.cancel_at <= self.clock() - t0:
+                    status = "cancelled"  # withdrawn mid-flight: slot and memory freed
                 elif self.check_energy:
                     e = run.energy(stream)
                     if not math.isfinite(e) or e / run.E0 > run.d.energy_thresh:
@@ -229,6 +236,9 @@ class KHServer:
             if footprint(req.cfg) > self.budget:
                 req.status = "rejected"
                 continue
+            if req.cancel_at <= self.clock() - t0:
+                req.status, req.finished = "cancelled", self.clock() - t0
+                continue
             now = self.clock() - t0
             if req.arrival > now:
                 time.sleep(req.arrival - now)
@@ -237,6 +247,9 @@ class KHServer:
             status = "done"
             left = req.steps
             while left > 0:
+                if req.cancel_at <= self.clock() - t0:
+                    status = "cancelled"
+                    break
                 k = min(self.chunk, left)
                 run.step(k, stream)
                 left -= k
