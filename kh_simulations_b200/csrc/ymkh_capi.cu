@@ -751,6 +751,13 @@ struct ymkh_batch {
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t gstream = nullptr;
   long long glaunches = 0;
+  // The members' column stages (z-mean, band filters, ...) are independent
+  // run to run: they fork onto auxiliary streams after the fused launches
+  // and join back before the next step (also inside a captured graph).
+  static constexpr int kAux = 8;
+  cudaStream_t aux[kAux]{};
+  cudaEvent_t fork_ev = nullptr;
+  cudaEvent_t join_ev[kAux]{};
 };
 
 namespace {
@@ -818,10 +825,22 @@ int batch_step_once(ymkh_batch* b, cudaStream_t s) {
     CK(launch_fct_table(T, b->tb, b->fct_grid, s), "fct_fused_kernel (batch)");
   CK(launch_maxwell_table(T, b->mx_grid, s), "maxwell_fused_kernel (batch)");
   g_launches += 2;
-  for (ymkh_ctx* c : b->runs) {
-    int rc = post_stages(c, c->buf[1 - c->cur], s);
+  const int na = b->aux[0] ? std::min(n, (int)ymkh_batch::kAux) : 1;
+  if (na > 1) {
+    CK(cudaEventRecord(b->fork_ev, s), "batch fork");
+    for (int i = 0; i < na; ++i) CK(cudaStreamWaitEvent(b->aux[i], b->fork_ev, 0), "batch fork");
+  }
+  for (int j = 0; j < n; ++j) {
+    ymkh_ctx* c = b->runs[j];
+    int rc = post_stages(c, c->buf[1 - c->cur], na > 1 ? b->aux[j % na] : s);
     if (rc) return rc;
     c->cur = 1 - c->cur;
+  }
+  if (na > 1) {
+    for (int i = 0; i < na; ++i) {
+      CK(cudaEventRecord(b->join_ev[i], b->aux[i]), "batch join");
+      CK(cudaStreamWaitEvent(s, b->join_ev[i], 0), "batch join");
+    }
   }
   b->parity ^= 1;
   return 0;
@@ -842,9 +861,19 @@ int ymkh_batch_create(ymkh_batch** out) {
   b->mx_grid = sms * std::max(1, maxwell_ctas_per_sm());
   b->fx_grid = sms * std::max(1, fct_split_ctas_per_sm(0)) * 4;
   b->fz_grid = sms * std::max(1, fct_split_ctas_per_sm(1)) * 4;
-  if (cudaMalloc(&b->derr, sizeof(unsigned)) != cudaSuccess || cudaMemset(b->derr, 0, sizeof(unsigned)) != cudaSuccess) {
+  bool ok = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming) == cudaSuccess;
+  for (int i = 0; ok && i < ymkh_batch::kAux; ++i)
+    ok = cudaStreamCreateWithFlags(&b->aux[i], cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&b->join_ev[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok || cudaMalloc(&b->derr, sizeof(unsigned)) != cudaSuccess ||
+      cudaMemset(b->derr, 0, sizeof(unsigned)) != cudaSuccess) {
+    for (int i = 0; i < ymkh_batch::kAux; ++i) {
+      if (b->aux[i]) cudaStreamDestroy(b->aux[i]);
+      if (b->join_ev[i]) cudaEventDestroy(b->join_ev[i]);
+    }
+    if (b->fork_ev) cudaEventDestroy(b->fork_ev);
     delete b;
-    return set_err(YMKH_ENOMEM, "cudaMalloc batch error word");
+    return set_err(YMKH_ENOMEM, "batch streams, events or error word");
   }
   *out = b;
   return 0;
@@ -956,6 +985,11 @@ int ymkh_batch_destroy(ymkh_batch* b) {
   batch_drop_graph(b);
   if (b->ddesc) cudaFree(b->ddesc);
   if (b->derr) cudaFree(b->derr);
+  for (int i = 0; i < ymkh_batch::kAux; ++i) {
+    if (b->aux[i]) cudaStreamDestroy(b->aux[i]);
+    if (b->join_ev[i]) cudaEventDestroy(b->join_ev[i]);
+  }
+  if (b->fork_ev) cudaEventDestroy(b->fork_ev);
   delete b;
   return 0;
 }
