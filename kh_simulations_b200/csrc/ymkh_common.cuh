@@ -47,12 +47,6 @@ __device__ __forceinline__ void fct_nu_mu(double eps, double& nu, double& mu) {
   nu = (1.0 / 6.0) + (1.0 / 3.0) * (eps * eps - scrh * scrh);
   mu = 0.25 - 0.5 * nu;
 }
-// FCT_DeviceMath.cuh:108-125 (apply_fct_limiter)
-__device__ __forceinline__ double fct_limit(double f, double dm1, double d0, double dp1) {
-  double s = copysign(1.0, d0);
-  double term = s * dm1, terp = s * dp1, fa = fabs(f);
-  return s * fmax(0.0, fmin(term, fmin(fa, terp)));
-}
 
 // Periodic / clamped index maps of the shear axis (ymgpu2d/YM_FCT.cu:7-18 pad,
 // FCT_Sweeps.cu:68-81 clamped halo loads).
@@ -112,7 +106,6 @@ cudaError_t prepare_fct(int tb);
 int fct_ctas_per_sm(int tb);
 cudaError_t prepare_maxwell();
 int maxwell_ctas_per_sm();
-int maxwell_strip_width();
 cudaError_t launch_sponge_xicut(const ArrayList& a12, const StepParams& p, int cut, cudaStream_t s);
 cudaError_t prepare_column(int nz);
 cudaError_t launch_zmean(const ArrayList& a15, int nx, int nz, cudaStream_t s);

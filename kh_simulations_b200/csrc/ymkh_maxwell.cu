@@ -285,8 +285,6 @@ int maxwell_ctas_per_sm() {
   return n;
 }
 
-int maxwell_strip_width() { return MX_TX; }
-
 int maxwell_nstrips(int nx) { return (nx + MX_TX - 1) / MX_TX; }
 
 int maxwell_bulk_ok(const StepParams& p) { return (p.periodic_x && (p.nx % 2) == 0 && p.nx >= MX_W) ? 1 : 0; }
