@@ -112,6 +112,7 @@ void fill_step_params(ymkh_ctx* c) {
   StepParams& s = c->sp;
   s.nx = c->nx; s.nz = c->nz;
   s.dx = p.dx; s.dz = p.dz; s.dt = p.dt_step;
+  s.rdx = 1.0 / p.dx; s.rdz = 1.0 / p.dz;  // IEEE division: correctly rounded
   s.c2 = p.c * p.c; s.eps0 = p.eps_0; s.alpha = p.alpha_YM;
   s.freeze_az1 = p.freeze_az1; s.periodic_x = p.periodic_x;
   s.epsilon = p.epsilon; s.xi_sponge = p.xi_sponge; s.sigma_sponge = p.sigma_sponge;

@@ -183,8 +183,8 @@ __global__ void __launch_bounds__(MX_NT, 4)
           for (int a = 0; a < 3; ++a) nq[b][a] = 0.5 * (n0 * fl[(FQ1 + a) * W + k] + n1 * fl[(FQ1 + a) * W + k + 1]);
         }
         const double by1 = sb[(MS_BY + 0) * W + k], by2 = sb[(MS_BY + 1) * W + k], by3 = sb[(MS_BY + 2) * W + k];
-        const double dz3[3] = {(by1 - sp[(MS_BY + 0) * W + k]) / p.dz, (by2 - sp[(MS_BY + 1) * W + k]) / p.dz,
-                               (by3 - sp[(MS_BY + 2) * W + k]) / p.dz};
+        const double dz3[3] = {div_rn(by1 - sp[(MS_BY + 0) * W + k], p.dz, p.rdz), div_rn(by2 - sp[(MS_BY + 1) * W + k], p.dz, p.rdz),
+                               div_rn(by3 - sp[(MS_BY + 2) * W + k], p.dz, p.rdz)};
         const double a1 = sb[(MS_AZ + 0) * W + k], a2 = sb[(MS_AZ + 1) * W + k], a3 = sb[(MS_AZ + 2) * W + k];
         const double kx[3] = {a2 * by3 - a3 * by2, a3 * by1 - a1 * by3, a1 * by2 - a2 * by1};
 #pragma unroll
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(MX_NT, 4)
           for (int a = 0; a < 3; ++a) {
             const double jz = -(nqz[0][a] * vzt[0] + nqz[1][a] * vzt[1]);
             const double by = sp[(MS_BY + a) * W + k];
-            const double dbx = (by - sp[(MS_BY + a) * W + k - 1]) / p.dx;
+            const double dbx = div_rn(by - sp[(MS_BY + a) * W + k - 1], p.dx, p.rdx);
             const double ez0 = wz ? 0.0 : sp[(MS_EZ + a) * W + k];
             wk[(MW_EZ + a) * W + k] = ez0 + dt * (unit ? dbx - jz : c2 * dbx - jz / e0);
           }
@@ -256,8 +256,8 @@ __global__ void __launch_bounds__(MX_NT, 4)
                                 az[0] * ex[1] - az[1] * ex[0]};
 #pragma unroll
           for (int a = 0; a < 3; ++a) {
-            const double dex = (wk[(MW_EX + rq * 3 + a) * W + k] - ex[a]) / p.dz;
-            const double dez = (wk[(MW_EZ + a) * W + k + 1] - ez[a]) / p.dx;
+            const double dex = div_rn(wk[(MW_EX + rq * 3 + a) * W + k] - ex[a], p.dz, p.rdz);
+            const double dez = div_rn(wk[(MW_EZ + a) * W + k + 1] - ez[a], p.dx, p.rdx);
             out.f[BY1 + a][gi] = sp[(MS_BY + a) * W + k] - dt * (dex - dez - al * kk[a]);
             out.f[AZ1 + a][gi] = az[a];
           }
