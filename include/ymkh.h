@@ -24,7 +24,8 @@
  *    exception crosses this boundary.
  *  - Streams: `stream` is a cudaStream_t passed as void*; NULL = legacy
  *    default stream (what the reference uses).  Every call is stream-ordered;
- *    only ymkh_energy / ymkh_mode_amp (host results) synchronise the stream.
+ *    only the calls with host results (ymkh_energy, ymkh_mode_amp,
+ *    ymkh_circ_amp, ymkh_gauss, ymkh_check) synchronise the stream.
  *  - Threading: one context per host thread at a time.
  */
 #ifndef YMKH_H
@@ -181,6 +182,47 @@ int ymkh_energy_async(ymkh_ctx* ctx, double* dev_out, void* stream);
  * out[0] = mean_x |sum_z (Az2 + i Az3) e^{-2 pi i k z / NZ}| / NZ,
  * out[1] = the same for the conjugate signal (Az2 - i Az3). */
 int ymkh_mode_amp(ymkh_ctx* ctx, int k, double* host_out2, void* stream);
+
+/* Colour-2/3 pairs of ymkh_circ_amp. */
+enum { YMKH_PAIR_AZ = 0, YMKH_PAIR_BY = 1, YMKH_PAIR_EX = 2, YMKH_PAIR_EZ = 3 };
+
+/* Circular mode amplitude of a colour-2/3 pair (F2 + i F3, F one of Az, By,
+ * Ex, Ez) at wavenumber k along z.  With host_weight NULL, the x-mean of
+ * ymkh_mode_amp; with NX weights, out[0] = sum_x w[x] |F_k(x)| / NZ and out[1]
+ * the same for F2 - i F3: the shear-layer weighted amplitude of
+ * ymgpu2d/analysis/resolution_convergence.py:77-86 (there from CSV snapshots,
+ * with w = sech((x - LX/2)/EPS) normalised).  Synchronises `stream`. */
+int ymkh_circ_amp(ymkh_ctx* ctx, int pair, int k, const double* host_weight, double* host_out2, void* stream);
+
+/* Non-Abelian Gauss law G^a = dEx^a/dx + dEz^a/dz + alpha (Az x Ez)^a - rho^a
+ * of ymgpu2d/analysis/gauss_check.py:40-110 (offline there, from CSV
+ * snapshots), on the current state: Yee differences with periodic wrap in x
+ * and z, Ez averaged to the cell centre, rho^a = Q^a_A nA + Q^a_B nB, and the
+ * state's own Az1.  host_out receives YMKH_GAUSS_NOUT root-mean-squares over
+ * the grid: [0..2] G^a, [3..5] div E^a, [6..8] alpha (Az x Ez)^a,
+ * [9..11] rho^a, [12..14] div E^a + alpha (Az x Ez)^a, [15] |Ex1|+..+|Ez3|.
+ * Synchronises `stream`. */
+#define YMKH_GAUSS_NOUT 16
+int ymkh_gauss(ymkh_ctx* ctx, double* host_out, void* stream);
+
+/* Snapshots of the current state (ymgpu2d/main_ym.cu:260-313).  The call
+ * enqueues the device-to-host copies on `stream` and returns; a writer
+ * thread waits for them and writes the file, at most 4 writers at a time
+ * (the oldest is joined first, as in the reference).
+ *  YMKH_SNAP_CSV:  the reference's 26-column CSV, byte for byte: header
+ *                  X,Z,By1,By2,By3,Az2,Az3,PzA,PxA,Q1A,PzB,PxB,Q1B,Ex1,Ex2,Ex3,
+ *                  Ez1,Ez2,Ez3,nA,nB,Q2A,Q3A,Q2B,Q3B,Az1; rows z-major, x
+ *                  fastest; X = x*dx, Z = z*dz; every value as printf "%g".
+ *  YMKH_SNAP_FP64: exact binary: a 40-byte header (char[8] "YMKHSNP1",
+ *                  uint32 version 1, nx, nz, narrays = 24, double dx, dz)
+ *                  then the 24 arrays in state order, native byte order.
+ * The copies read the state at their place in `stream`'s order: work that
+ * changes the state on another stream must wait for `stream`.  Errors of a
+ * writer (file cannot be opened or written) are returned by the next
+ * ymkh_snapshot or ymkh_snapshot_wait.  ymkh_destroy waits too. */
+enum { YMKH_SNAP_CSV = 0, YMKH_SNAP_FP64 = 1 };
+int ymkh_snapshot(ymkh_ctx* ctx, const char* path, int format, void* stream);
+int ymkh_snapshot_wait(ymkh_ctx* ctx);
 
 /* Reports (and clears) a failure of the bounded waits inside the kernels
  * (a staged row that never arrived): YMKH_ECUDA if one timed out since the

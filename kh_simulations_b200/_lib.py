@@ -16,6 +16,9 @@ MAX_EXTRA_BANDS = 4
 NOALLOC_MAX_CELLS = 134217728  # YMKH_NOALLOC_MAX_CELLS
 FILTER_DFT, FILTER_TF32X3 = 0, 1
 FCT_FUSED, FCT_SPLIT = 0, 1
+PAIRS = {"Az": 0, "By": 1, "Ex": 2, "Ez": 3}  # YMKH_PAIR_*
+GAUSS_NOUT = 16  # YMKH_GAUSS_NOUT
+SNAP_CSV, SNAP_FP64 = 0, 1
 
 # state order of include/ymkh.h
 STATE_NAMES = (
@@ -84,6 +87,10 @@ _SIGS = {
     "ymkh_energy": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
     "ymkh_energy_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "ymkh_mode_amp": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_void_p]),
+    "ymkh_circ_amp": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
+    "ymkh_gauss": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
+    "ymkh_snapshot": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_void_p]),
+    "ymkh_snapshot_wait": (C.c_int, [C.c_void_p]),
     "ymkh_destroy": (C.c_int, [C.c_void_p]),
     "ymkh_check": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ymkh_batch_create": (C.c_int, [C.POINTER(C.c_void_p)]),

@@ -82,6 +82,9 @@ struct ymkh_ctx {
   double* epart = nullptr;   // energy partials
   double* edev = nullptr;    // [0] energy, [1..2] mode amplitudes
   double* mcol = nullptr;    // mode amplitude per-column buffer
+  double* mweight = nullptr; // x weights of ymkh_circ_amp (NX doubles, allocated on first use)
+  double* gpart = nullptr;   // Gauss residual partials and results (allocated on first use)
+  SnapshotQueue* snaps = nullptr;  // snapshot writers (created on first use)
   int fct_tx = 64, fct_seg = 16, fct_grid = 296;  // FCT threads per beam, segment rows, persistent CTAs
   int mx_seg = 16, mx_grid = 148;                   // Maxwell segment rows, persistent CTAs
   int sms = 148;
@@ -691,25 +694,79 @@ int ymkh_energy(ymkh_ctx* c, double* host_out, void* stream) {
 }
 
 int ymkh_mode_amp(ymkh_ctx* c, int k, double* host_out2, void* stream) {
+  return ymkh_circ_amp(c, YMKH_PAIR_AZ, k, nullptr, host_out2, stream);
+}
+
+int ymkh_circ_amp(ymkh_ctx* c, int pair, int k, const double* host_weight, double* host_out2, void* stream) {
   if (!c || !host_out2) return set_err(YMKH_EINVAL, "null argument");
   if (!c->bound) return set_err(YMKH_ESTATE, "state not bound");
+  static const int re_of[4] = {AZ2, BY2, EX2, EZ2};
+  if (pair < 0 || pair > 3) return set_err(YMKH_EINVAL, "pair %d not in 0..3", pair);
   cudaStream_t s = (cudaStream_t)stream;
   const State& st = c->buf[c->cur];
-  CK(launch_mode_amp(st.f[AZ2], st.f[AZ3], c->nx, c->nz, k, c->mcol, c->edev + 1, s), "mode amplitude kernels");
+  const double* w = nullptr;
+  if (host_weight) {
+    if (!c->mweight && cudaMalloc(&c->mweight, (size_t)c->nx * sizeof(double)) != cudaSuccess)
+      return set_err(YMKH_ENOMEM, "cudaMalloc mode weights");
+    CK(cudaMemcpyAsync(c->mweight, host_weight, (size_t)c->nx * sizeof(double), cudaMemcpyHostToDevice, s),
+       "mode weights H2D");
+    w = c->mweight;
+  }
+  CK(launch_mode_amp(st.f[re_of[pair]], st.f[re_of[pair] + 1], c->nx, c->nz, k, c->mcol, w, c->edev + 1, s),
+     "mode amplitude kernels");
   g_launches += 2;
   CK(cudaMemcpyAsync(host_out2, c->edev + 1, 2 * sizeof(double), cudaMemcpyDeviceToHost, s), "mode amp D2H");
   CK(cudaStreamSynchronize(s), "mode amp sync");
   return 0;
 }
 
+int ymkh_gauss(ymkh_ctx* c, double* host_out, void* stream) {
+  if (!c || !host_out) return set_err(YMKH_EINVAL, "null argument");
+  if (!c->bound) return set_err(YMKH_ESTATE, "state not bound");
+  const int np = gauss_nparts(c->N);
+  const size_t n = (size_t)np * YMKH_GAUSS_NOUT * 2 + YMKH_GAUSS_NOUT;
+  if (!c->gpart && cudaMalloc(&c->gpart, n * sizeof(double)) != cudaSuccess)
+    return set_err(YMKH_ENOMEM, "cudaMalloc Gauss partials");
+  cudaStream_t s = (cudaStream_t)stream;
+  double* dout = c->gpart + (size_t)np * YMKH_GAUSS_NOUT * 2;
+  CK(launch_gauss(c->buf[c->cur], c->nx, c->nz, c->prm.dx, c->prm.dz, c->prm.alpha_YM, c->gpart, dout, s),
+     "Gauss residual kernels");
+  g_launches += 2;
+  CK(cudaMemcpyAsync(host_out, dout, YMKH_GAUSS_NOUT * sizeof(double), cudaMemcpyDeviceToHost, s), "Gauss D2H");
+  CK(cudaStreamSynchronize(s), "Gauss sync");
+  return 0;
+}
+
+int ymkh_snapshot(ymkh_ctx* c, const char* path, int format, void* stream) {
+  if (!c || !path) return set_err(YMKH_EINVAL, "null argument");
+  if (!c->bound) return set_err(YMKH_ESTATE, "state not bound");
+  if (format != YMKH_SNAP_CSV && format != YMKH_SNAP_FP64) return set_err(YMKH_EINVAL, "snapshot format %d", format);
+  if (!c->snaps) c->snaps = snapshot_queue_create(c->device);
+  std::string err;
+  const int rc = snapshot_submit(c->snaps, c->buf[c->cur], c->nx, c->nz, c->prm.dx, c->prm.dz, path, format,
+                                 (cudaStream_t)stream, err);
+  return rc ? set_err(rc, "%s", err.c_str()) : 0;
+}
+
+int ymkh_snapshot_wait(ymkh_ctx* c) {
+  if (!c) return set_err(YMKH_EINVAL, "null context");
+  if (!c->snaps) return 0;
+  std::string err;
+  const int rc = snapshot_wait(c->snaps, err);
+  return rc ? set_err(rc, "%s", err.c_str()) : 0;
+}
+
 int ymkh_destroy(ymkh_ctx* c) {
   if (!c) return 0;
+  if (c->snaps) snapshot_queue_destroy(c->snaps);  // waits for its writers
   drop_graphs(c);
   free_bands(c);
   if (c->own) cudaFree(c->own);
   if (c->epart) cudaFree(c->epart);
   if (c->edev) cudaFree(c->edev);
   if (c->mcol) cudaFree(c->mcol);
+  if (c->mweight) cudaFree(c->mweight);
+  if (c->gpart) cudaFree(c->gpart);
   if (c->derr) cudaFree(c->derr);
   if (c->ddesc) cudaFree(c->ddesc);
   if (c->xscratch) cudaFree(c->xscratch);

@@ -284,15 +284,6 @@ cudaError_t launch_band(const ArrayList& arrs, int narr, const double* W, int ld
 // Per-cell energy of YM_Energy.cu:3-21, summed with Neumaier compensation in
 // a fixed order: each CTA reduces a contiguous block of cells, a second
 // single-CTA pass reduces the CTA partials in index order.
-__device__ __forceinline__ void neumaier_add(double& s, double& c, double v) {
-  const double t = s + v;
-  if (fabs(s) >= fabs(v))
-    c += (s - t) + v;
-  else
-    c += (v - t) + s;
-  s = t;
-}
-
 constexpr int EN_THREADS = 256;
 constexpr int EN_PER_THREAD = 16;
 
@@ -376,10 +367,10 @@ cudaError_t launch_energy(const State& st, size_t N, double* part, double* out, 
 }
 
 // ------------------------------------------------------------ mode amplitude
-// ymgpu2d/analysis/remote_timeseries.py:62-77: per column x,
-// F = sum_z (Az2 + i Az3) e^{-2 pi i k z/nz}, Fc for Az2 - i Az3;
-// out = (mean_x |F| / nz, mean_x |Fc| / nz).
-__global__ void mode_amp_kernel(const double* __restrict__ az2, const double* __restrict__ az3, int nx, int nz,
+// Per column x, F = sum_z (re + i im) e^{-2 pi i k z/nz} and Fc for re - i im
+// (ymgpu2d/analysis/remote_timeseries.py:62-77 for re, im = Az2, Az3;
+// ymgpu2d/analysis/resolution_convergence.py:83-86 for By2, By3).
+__global__ void mode_amp_kernel(const double* __restrict__ re, const double* __restrict__ im, int nx, int nz,
                                 int k, double* __restrict__ colbuf) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= nx) return;
@@ -387,7 +378,7 @@ __global__ void mode_amp_kernel(const double* __restrict__ az2, const double* __
   for (int z = 0; z < nz; ++z) {
     double sn, cs;
     sincospi(-2.0 * (double)k * (double)z / (double)nz, &sn, &cs);
-    const double a = az2[idx2(x, z, nx)], b = az3[idx2(x, z, nx)];
+    const double a = re[idx2(x, z, nx)], b = im[idx2(x, z, nx)];
     // (a + i b)(cs + i sn)
     fr += a * cs - b * sn;
     fi += a * sn + b * cs;
@@ -399,23 +390,36 @@ __global__ void mode_amp_kernel(const double* __restrict__ az2, const double* __
   colbuf[2 * x + 1] = hypot(cr, ci);
 }
 
-__global__ void mode_amp_final_kernel(const double* __restrict__ colbuf, int nx, int nz, double* out) {
+// Without a weight: (mean_x |F| / nz, mean_x |Fc| / nz), remote_timeseries.py:72-74.
+// With one: (sum_x w[x] |F| / nz, sum_x w[x] |Fc| / nz), the shear-layer
+// weighted average of resolution_convergence.py:83-86.
+__global__ void mode_amp_final_kernel(const double* __restrict__ colbuf, const double* __restrict__ w, int nx, int nz,
+                                      double* out) {
   if (threadIdx.x != 0) return;
   double s0 = 0, s1 = 0;
-  for (int x = 0; x < nx; ++x) {
-    s0 += colbuf[2 * x];
-    s1 += colbuf[2 * x + 1];
+  if (w == nullptr) {
+    for (int x = 0; x < nx; ++x) {
+      s0 += colbuf[2 * x];
+      s1 += colbuf[2 * x + 1];
+    }
+    out[0] = s0 / nx / nz;
+    out[1] = s1 / nx / nz;
+  } else {
+    for (int x = 0; x < nx; ++x) {
+      s0 += w[x] * (colbuf[2 * x] / nz);
+      s1 += w[x] * (colbuf[2 * x + 1] / nz);
+    }
+    out[0] = s0;
+    out[1] = s1;
   }
-  out[0] = s0 / nx / nz;
-  out[1] = s1 / nx / nz;
 }
 
-cudaError_t launch_mode_amp(const double* az2, const double* az3, int nx, int nz, int k, double* colbuf, double* out,
-                            cudaStream_t s) {
-  mode_amp_kernel<<<(nx + 127) / 128, 128, 0, s>>>(az2, az3, nx, nz, k, colbuf);
+cudaError_t launch_mode_amp(const double* re, const double* im, int nx, int nz, int k, double* colbuf,
+                            const double* weight, double* out, cudaStream_t s) {
+  mode_amp_kernel<<<(nx + 127) / 128, 128, 0, s>>>(re, im, nx, nz, k, colbuf);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  mode_amp_final_kernel<<<1, 32, 0, s>>>(colbuf, nx, nz, out);
+  mode_amp_final_kernel<<<1, 32, 0, s>>>(colbuf, weight, nx, nz, out);
   return cudaGetLastError();
 }
 

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <algorithm>
+#include <string>
 #include "../../include/ymkh.h"
 
 namespace ymkh {
@@ -34,6 +35,18 @@ struct StepParams {
 
 __host__ __device__ __forceinline__ size_t idx2(int x, int z, int nx) {
   return (size_t)x + (size_t)z * (size_t)nx;
+}
+
+// s + c += v, Neumaier's compensated summation (A. Neumaier, "Rundungsfehleranalyse
+// einiger Verfahren zur Summation endlicher Summen", ZAMM 54, 1974): c gathers the
+// rounding error of every addition to s.
+__device__ __forceinline__ void neumaier_add(double& s, double& c, double v) {
+  const double t = s + v;
+  if (fabs(s) >= fabs(v))
+    c += (s - t) + v;
+  else
+    c += (v - t) + s;
+  s = t;
 }
 
 // FCT_DeviceMath.cuh:38-46 (compute_eps)
@@ -137,8 +150,20 @@ cudaError_t launch_twiddles(double* W, int nz, int lo, int hi, int ldw, cudaStre
 cudaError_t launch_twiddles_f32(float* c, float* sn, int nz, int lo, int hi, cudaStream_t s);
 cudaError_t launch_energy(const State& st, size_t N, double* part, double* out, cudaStream_t s);
 int energy_nparts(size_t N);
-cudaError_t launch_mode_amp(const double* az2, const double* az3, int nx, int nz, int k, double* colbuf, double* out,
-                            cudaStream_t s);
+cudaError_t launch_mode_amp(const double* re, const double* im, int nx, int nz, int k, double* colbuf,
+                            const double* weight, double* out, cudaStream_t s);
+// State snapshots written by host threads (ymkh_snapshot.cu).
+class SnapshotQueue;
+SnapshotQueue* snapshot_queue_create(int device);
+void snapshot_queue_destroy(SnapshotQueue* q);
+int snapshot_submit(SnapshotQueue* q, const State& st, int nx, int nz, double dx, double dz, const char* path,
+                    int format, cudaStream_t s, std::string& err);
+int snapshot_wait(SnapshotQueue* q, std::string& err);
+// Non-Abelian Gauss law residual sums (ymkh_diag.cu); part holds
+// gauss_nparts(N) * YMKH_GAUSS_NOUT * 2 doubles, out YMKH_GAUSS_NOUT.
+int gauss_nparts(size_t N);
+cudaError_t launch_gauss(const State& st, int nx, int nz, double dx, double dz, double alpha, double* part,
+                         double* out, cudaStream_t s);
 cudaError_t launch_init(const State& st, const InitArgs& a, cudaStream_t s);
 // 3-pass TF32 band filter on the tensor cores (ymkh_tf32.cu).  Per band:
 // the twiddle matrix as TF32 hi/lo tile images for both contractions;

@@ -3,8 +3,9 @@
 Replaces the driver ymgpu2d/main_ym.cu: configuration and derivation
 (:24-83), allocation (:85-121, here two 24-array FP64 buffers held as torch
 tensors), seed profile upload (:178-217), initial state (:219-237), the
-step loop with the energy check and halt rules (:318-479) and
-``energy.csv`` in the reference's format (:251-256, :458-466).
+step loop with the energy check and halt rules (:318-479), ``energy.csv``
+in the reference's format (:251-256, :458-466) and the state snapshots
+(:260-313, :476-477).
 The arithmetic runs in the CUDA library (include/ymkh.h); this module only
 owns memory, streams and files.
 """
@@ -19,7 +20,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import NSTATE, STATE_NAMES, Grid, InitParams, check
+from ._lib import GAUSS_NOUT, NSTATE, PAIRS, SNAP_CSV, SNAP_FP64, STATE_NAMES, Grid, InitParams, check
 from .config import Derived, RunConfig, derive, load_config, step_params
 from .seed import load_profiles
 
@@ -164,17 +165,74 @@ class KHRun:
             check(self.lib.ymkh_mode_amp(self.ctx, int(k), out, C.c_void_p(_stream_ptr(stream))), "ymkh_mode_amp")
         return out[0], out[1]
 
+    def circ_amp(self, pair: str = "Az", k: int | None = None, weight=None, stream=None) -> tuple:
+        """(|F2 + i F3|_k, |F2 - i F3|_k) averaged over x for F in Az, By, Ex,
+        Ez: the plain mean, or the sum weighted by ``weight`` (NX values,
+        e.g. growth.xi_weight, as in ymgpu2d/analysis/resolution_convergence.py:77-86)."""
+        out = (C.c_double * 2)()
+        k = self.cfg.k_mode if k is None else k
+        w = None
+        if weight is not None:
+            w = np.ascontiguousarray(weight, dtype=np.float64)
+            if w.shape != (self.d.nx,):
+                raise ValueError(f"weight has shape {w.shape}, expected ({self.d.nx},)")
+        with torch.cuda.device(self.device):
+            check(self.lib.ymkh_circ_amp(self.ctx, PAIRS[pair], int(k), None if w is None else w.ctypes.data, out,
+                                         C.c_void_p(_stream_ptr(stream))), "ymkh_circ_amp")
+        return out[0], out[1]
+
+    def gauss(self, stream=None) -> dict:
+        """Root-mean-square terms of the non-Abelian Gauss law on the current
+        state (ymgpu2d/analysis/gauss_check.py:40-110 and its summary):
+        arrays of the three colours for G, div_E, nonabelian, rho and lhs
+        (div_E + nonabelian), and Etot_scale = rms(|Ex|+|Ez| summed over
+        colours) / dx + 1e-30, the scale of its relative error."""
+        out = (C.c_double * GAUSS_NOUT)()
+        with torch.cuda.device(self.device):
+            check(self.lib.ymkh_gauss(self.ctx, out, C.c_void_p(_stream_ptr(stream))), "ymkh_gauss")
+        v = np.array(out[:], dtype=np.float64)
+        return {"G": v[0:3], "div_E": v[3:6], "nonabelian": v[6:9], "rho": v[9:12], "lhs": v[12:15],
+                "Etot_scale": v[15] / self.d.dx + 1e-30}
+
+    def snapshot(self, path: str | Path, fmt: str = "csv", stream=None) -> None:
+        """Write the current state to ``path`` in the background: ``csv`` is
+        the reference's 26-column snapshot, ``fp64`` the exact binary form
+        (include/ymkh.h, ymkh_snapshot).  snapshot_wait() joins the writers."""
+        f = {"csv": SNAP_CSV, "fp64": SNAP_FP64}[fmt]
+        with torch.cuda.device(self.device):
+            check(self.lib.ymkh_snapshot(self.ctx, str(path).encode(), f, C.c_void_p(_stream_ptr(stream))),
+                  "ymkh_snapshot")
+
+    def snapshot_wait(self) -> None:
+        check(self.lib.ymkh_snapshot_wait(self.ctx), "ymkh_snapshot_wait")
+
     # ------------------------------------------------------------------ loop
     def run(self, total_steps: int | None = None, energy_stride: int | None = None, csv: str | Path | None = None,
-            on_energy=None, stream=None, mode_amp: bool = False) -> list:
-        """The time loop of ymgpu2d/main_ym.cu:318-479 (without CSV snapshots):
-        energy every ``energy_stride`` steps, halt on NaN/Inf or E/E0 above
-        the reference's threshold (:249, :467-474).  With mode_amp, the
-        k_mode amplitude (offline in the reference,
-        analysis/remote_timeseries.py:62-77) is recorded at the same stride."""
+            on_energy=None, stream=None, mode_amp: bool = False, export_dir: str | Path | None = None,
+            export_format: str = "csv", export_stride: int | None = None, on_export=None) -> list:
+        """The time loop of ymgpu2d/main_ym.cu:318-479: energy every
+        ``energy_stride`` steps, halt on NaN/Inf or E/E0 above the
+        reference's threshold (:249, :467-474).  With mode_amp, the k_mode
+        amplitude (offline in the reference,
+        analysis/remote_timeseries.py:62-77) is recorded at the same stride.
+        Every ``export_stride`` steps (and at step 0), after the energy
+        check, the state is exported (:476-477): written to
+        ``export_dir/ym_%06d.csv`` (or ``.fp64``) when export_dir is given,
+        and passed to ``on_export(run, step)`` when that is given."""
         d = self.d
         total = d.total_steps if total_steps is None else total_steps
         stride = d.energy_stride if energy_stride is None else energy_stride
+        xstride = d.export_stride if export_stride is None else export_stride
+        exporting = export_dir is not None or on_export is not None
+        if export_dir is not None:
+            Path(export_dir).mkdir(parents=True, exist_ok=True)
+
+        def export(step):
+            if export_dir is not None:
+                self.snapshot(Path(export_dir) / f"ym_{step:06d}.{export_format}", export_format, stream)
+            if on_export:
+                on_export(self, step)
+
         fh = open(csv, "w") if csv else None
         try:
             if self.E0 is None:
@@ -184,8 +242,12 @@ class KHRun:
                 if fh:
                     fh.write("step,time,E_total,E_ratio\n")
                     fh.write(f"0,0,{self.E0:.8e},1.0\n")
+                if exporting and self.step_count == 0:
+                    export(0)
             while self.step_count < total and not self.halted:
                 n = min(stride - (self.step_count % stride), total - self.step_count)
+                if exporting:
+                    n = min(n, xstride - (self.step_count % xstride))
                 self.step(n, stream)
                 if self.step_count % stride == 0:
                     E = self.energy(stream)
@@ -203,9 +265,13 @@ class KHRun:
                         self.halted, self.halt_reason = True, f"NaN/Inf at t={t}"
                     elif ratio > d.energy_thresh:
                         self.halted, self.halt_reason = True, f"E/E0={ratio} > {d.energy_thresh} at t={t}"
+                if exporting and self.step_count % xstride == 0:
+                    export(self.step_count)
         finally:
             if fh:
                 fh.close()
+            if export_dir is not None:
+                self.snapshot_wait()
         return self.history
 
     # ------------------------------------------------------------ checkpoint
