@@ -186,3 +186,14 @@ def fit_growth_rate_plateau(times, amps, win_tu: float = 8.0, min_plateau_tu: fl
     t, a = times[m] - times[m].mean(), log_a[m] - log_a[m].mean()
     return {"gamma": float(np.dot(t, a) / np.dot(t, t)), "t0": float(t0), "t1": float(t1),
             "duration": float(best[2]), "has_plateau": True}
+
+
+def wkb_exact_gamma(alpha: float, V0: float, kz: float) -> float:
+    """Largest Im(omega) over the roots of the harmonic-core WKB quartic
+    omega^4 - kz^2 omega^2 - C omega - alpha^2 V0 kz = 0 with
+    C = sqrt(alpha^3 / 2) V0 (the fundamental mode), 0.0 when no root grows
+    (ymgpu2d/analysis/batch_analyze.py:19-41)."""
+    c = math.sqrt(alpha ** 3 / 2.0) * V0
+    roots = np.roots([1.0, 0.0, -kz ** 2, -c, -alpha ** 2 * V0 * kz])
+    growing = roots[roots.imag > 1e-8]
+    return float(np.max(growing.imag)) if len(growing) else 0.0

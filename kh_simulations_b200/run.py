@@ -219,59 +219,15 @@ class KHRun:
         check, the state is exported (:476-477): written to
         ``export_dir/ym_%06d.csv`` (or ``.fp64``) when export_dir is given,
         and passed to ``on_export(run, step)`` when that is given."""
-        d = self.d
-        total = d.total_steps if total_steps is None else total_steps
-        stride = d.energy_stride if energy_stride is None else energy_stride
-        xstride = d.export_stride if export_stride is None else export_stride
-        exporting = export_dir is not None or on_export is not None
-        if export_dir is not None:
-            Path(export_dir).mkdir(parents=True, exist_ok=True)
-
-        def export(step):
-            if export_dir is not None:
-                self.snapshot(Path(export_dir) / f"ym_{step:06d}.{export_format}", export_format, stream)
-            if on_export:
-                on_export(self, step)
-
-        fh = open(csv, "w") if csv else None
+        loop = RunLoop(self, total_steps, energy_stride, csv, on_energy, stream, mode_amp, export_dir, export_format,
+                       export_stride, on_export)
         try:
-            if self.E0 is None:
-                self.E0 = self.energy(stream)
-                amp0 = self.mode_amp(stream=stream)[0] if mode_amp else math.nan
-                self.history.append(EnergyRecord(0, 0.0, self.E0, 1.0, amp0))
-                if fh:
-                    fh.write("step,time,E_total,E_ratio\n")
-                    fh.write(f"0,0,{self.E0:.8e},1.0\n")
-                if exporting and self.step_count == 0:
-                    export(0)
-            while self.step_count < total and not self.halted:
-                n = min(stride - (self.step_count % stride), total - self.step_count)
-                if exporting:
-                    n = min(n, xstride - (self.step_count % xstride))
-                self.step(n, stream)
-                if self.step_count % stride == 0:
-                    E = self.energy(stream)
-                    ratio = E / self.E0
-                    t = self.step_count * d.dt
-                    amp = self.mode_amp(stream=stream)[0] if mode_amp else math.nan
-                    rec = EnergyRecord(self.step_count, t, E, ratio, amp)
-                    self.history.append(rec)
-                    if fh:
-                        fh.write(f"{self.step_count},{t:.8e},{E:.8e},{ratio:.8e}\n")
-                        fh.flush()
-                    if on_energy:
-                        on_energy(self, rec)
-                    if math.isnan(E) or math.isinf(E):
-                        self.halted, self.halt_reason = True, f"NaN/Inf at t={t}"
-                    elif ratio > d.energy_thresh:
-                        self.halted, self.halt_reason = True, f"E/E0={ratio} > {d.energy_thresh} at t={t}"
-                if exporting and self.step_count % xstride == 0:
-                    export(self.step_count)
+            loop.start()
+            while not loop.finished:
+                self.step(loop.steps_to_event(), stream)
+                loop.after_steps()
         finally:
-            if fh:
-                fh.close()
-            if export_dir is not None:
-                self.snapshot_wait()
+            loop.close()
         return self.history
 
     # ------------------------------------------------------------ checkpoint
@@ -319,3 +275,87 @@ class KHRun:
     @classmethod
     def from_ini(cls, path: str | Path, **kw) -> "KHRun":
         return cls(load_config(path), **kw)
+
+
+class RunLoop:
+    """The bookkeeping of ymgpu2d/main_ym.cu:318-479 for one run, with the
+    stepping left to the caller (``KHRun.run`` steps the run alone; a
+    campaign steps many runs in one batch).  ``steps_to_event`` says how
+    many steps may be taken before the next energy check, export or the
+    end; ``after_steps`` does what the reference does at the step reached:
+    energy check, energy.csv line, halt rule, then export."""
+
+    def __init__(self, run: KHRun, total_steps=None, energy_stride=None, csv=None, on_energy=None, stream=None,
+                 mode_amp=False, export_dir=None, export_format="csv", export_stride=None, on_export=None):
+        d = run.d
+        self.run = run
+        self.total = d.total_steps if total_steps is None else total_steps
+        self.stride = d.energy_stride if energy_stride is None else energy_stride
+        self.xstride = d.export_stride if export_stride is None else export_stride
+        self.stream = stream
+        self.mode_amp = mode_amp
+        self.on_energy = on_energy
+        self.on_export = on_export
+        self.export_dir = Path(export_dir) if export_dir is not None else None
+        self.export_format = export_format
+        self.exporting = export_dir is not None or on_export is not None
+        if self.export_dir is not None:
+            self.export_dir.mkdir(parents=True, exist_ok=True)
+        self.fh = open(csv, "w") if csv else None
+
+    @property
+    def finished(self) -> bool:
+        return self.run.step_count >= self.total or self.run.halted
+
+    def _export(self, step: int) -> None:
+        if self.export_dir is not None:
+            self.run.snapshot(self.export_dir / f"ym_{step:06d}.{self.export_format}", self.export_format, self.stream)
+        if self.on_export:
+            self.on_export(self.run, step)
+
+    def start(self) -> None:
+        run, fh = self.run, self.fh
+        if run.E0 is None:
+            run.E0 = run.energy(self.stream)
+            amp0 = run.mode_amp(stream=self.stream)[0] if self.mode_amp else math.nan
+            run.history.append(EnergyRecord(0, 0.0, run.E0, 1.0, amp0))
+            if fh:
+                fh.write("step,time,E_total,E_ratio\n")
+                fh.write(f"0,0,{run.E0:.8e},1.0\n")
+            if self.exporting and run.step_count == 0:
+                self._export(0)
+
+    def steps_to_event(self) -> int:
+        sc = self.run.step_count
+        n = min(self.stride - sc % self.stride, self.total - sc)
+        if self.exporting:
+            n = min(n, self.xstride - sc % self.xstride)
+        return n
+
+    def after_steps(self) -> None:
+        run, d, sc = self.run, self.run.d, self.run.step_count
+        if sc % self.stride == 0:
+            E = run.energy(self.stream)
+            ratio = E / run.E0
+            t = sc * d.dt
+            amp = run.mode_amp(stream=self.stream)[0] if self.mode_amp else math.nan
+            rec = EnergyRecord(sc, t, E, ratio, amp)
+            run.history.append(rec)
+            if self.fh:
+                self.fh.write(f"{sc},{t:.8e},{E:.8e},{ratio:.8e}\n")
+                self.fh.flush()
+            if self.on_energy:
+                self.on_energy(run, rec)
+            if math.isnan(E) or math.isinf(E):
+                run.halted, run.halt_reason = True, f"NaN/Inf at t={t}"
+            elif ratio > d.energy_thresh:
+                run.halted, run.halt_reason = True, f"E/E0={ratio} > {d.energy_thresh} at t={t}"
+        if self.exporting and sc % self.xstride == 0:
+            self._export(sc)
+
+    def close(self) -> None:
+        if self.fh:
+            self.fh.close()
+            self.fh = None
+        if self.export_dir is not None:
+            self.run.snapshot_wait()

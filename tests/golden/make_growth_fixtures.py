@@ -12,7 +12,8 @@ Inputs:
 - seeded synthetic histories (numpy default_rng(7)): exponential growth
   with saturation and noise, of several lengths.
 
-Outputs for every history: the reference's fit_growth_rate and
+Also the reference's WKB growth rate (batch_analyze.py:19-41) on a grid of
+(alpha, V0, kz).  Outputs for every history: the reference's fit_growth_rate and
 fit_growth_rate_plateau (ymgpu2d/analysis/batch_analyze.py:44-150) and its
 windowed fit (ymgpu2d/analysis/resolution_convergence.py:89-125), computed by
 importing those modules.  resolution_convergence imports matplotlib, which
@@ -80,8 +81,11 @@ def main():
     runs = {"res_baseline": {"nz_override": 256, "nx_override": 768, "courant_override": 0.01},
             "res_nz128": {"nz_override": 128, "nx_override": 384, "courant_override": 0.01},
             "res_c0.04": {"nz_override": 256, "nx_override": 768, "courant_override": 0.04}}
+    wkb = [[a, v, k, float(ba.wkb_exact_gamma(a, v, k))]
+           for a in (0.0, 0.1, 0.5, 1.0, 2.5, 6.0) for v in (0.01, 0.05, 0.2) for k in (0.125, 0.5, 1.0, 3.0, 7.0)]
     OUT.write_text(json.dumps({"source": "ymgpu2d/analysis/resconv_data.json + seeded synthetic histories",
-                               "t_min": 10.0, "physics": physics, "runs": runs, "cases": cases}, indent=1) + "\n")
+                               "t_min": 10.0, "physics": physics, "runs": runs, "cases": cases,
+                               "wkb_exact_gamma": wkb}, indent=1) + "\n")
     print(f"wrote {OUT} ({len(cases)} histories)")
 
 

@@ -74,3 +74,8 @@ def test_xi_weight_is_a_normalised_sech():
     w = growth.xi_weight(768, 6 * math.pi / 768, eps=0.15)
     assert w.sum() == pytest.approx(1.0, abs=1e-15)
     assert int(np.argmax(w)) == 384
+
+
+def test_wkb_exact_gamma_matches_the_reference():
+    for alpha, v0, kz, ref in FIX["wkb_exact_gamma"]:
+        assert growth.wkb_exact_gamma(alpha, v0, kz) == pytest.approx(ref, rel=1e-12, abs=1e-300), (alpha, v0, kz)
