@@ -94,12 +94,14 @@ class RunConfig:
     kz_keep_max: int = -1
     kz_bands: list = field(default_factory=list)
     filter_engine: str = "dft"
+    eigen_seed: int = 0       # 1: seed from the eigenmode solved at init (no seed file)
+    eigen_seed_nx: int = 384  # grid of that solve (the reference solver's default)
 
 
 FILTER_ENGINES = {"dft": 0, "tf32x3": 1}
 
 _INT_KEYS = {"k_mode", "run_mode", "freeze_override", "suppress_kz0", "kz_suppress_max", "kz_suppress_hi",
-             "init_by1_eq", "nz_override", "nx_override", "kz_keep_max"}
+             "init_by1_eq", "nz_override", "nx_override", "kz_keep_max", "eigen_seed", "eigen_seed_nx"}
 _STR_KEYS = {"run_tag", "seed_profile_file", "filter_engine"}
 _FLOAT_KEYS = {f.name for f in fields(RunConfig)} - _INT_KEYS - _STR_KEYS - {"kz_bands"}
 

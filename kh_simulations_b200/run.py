@@ -22,7 +22,7 @@ import torch
 from . import _lib
 from ._lib import GAUSS_NOUT, NSTATE, PAIRS, SNAP_CSV, SNAP_FP64, STATE_NAMES, Grid, InitParams, check
 from .config import Derived, RunConfig, derive, load_config, step_params
-from .seed import load_profiles
+from .seed import interpolate, load_profiles
 
 
 def init_params(cfg: RunConfig, d: Derived, profiles: dict | None = None):
@@ -122,11 +122,26 @@ class KHRun:
         return self.state.cpu().numpy()
 
     # ----------------------------------------------------------------- init
-    def init(self, seed_file: str | Path | None = None, stream=None) -> None:
-        """kernel_ym_init with the run's parameters (main_ym.cu:219-226)."""
+    def init(self, seed_file: str | Path | None = None, stream=None, seed_profiles: dict | None = None) -> None:
+        """kernel_ym_init with the run's parameters (main_ym.cu:219-226).
+
+        The seed profiles come from, in this order: ``seed_profiles`` (float32
+        profiles on any grid, as a seed file holds them), ``seed_file``,
+        the config's ``seed_profile_file``, or, with ``eigen_seed = 1``, the
+        eigenmode of the run's parameters solved here (eigenmode.py) as the
+        reference's offline solver would write it.  Profiles are interpolated
+        to the run's grid as the reference interpolates a seed file."""
         cfg, d = self.cfg, self.d
         seed_file = seed_file if seed_file is not None else (cfg.seed_profile_file or None)
-        ip, keep = init_params(cfg, d, load_profiles(seed_file, d.nx) if seed_file else None)
+        if seed_profiles is None and seed_file is None and cfg.eigen_seed:
+            from . import eigenmode
+
+            seed_profiles = eigenmode.cached_seed(eigenmode.spec_for_run(cfg, d, cfg.eigen_seed_nx))
+        if seed_profiles is not None:
+            profiles = {k: interpolate(v, d.nx) for k, v in seed_profiles.items()}
+        else:
+            profiles = load_profiles(seed_file, d.nx) if seed_file else None
+        ip, keep = init_params(cfg, d, profiles)
         with torch.cuda.device(self.device):
             check(self.lib.ymkh_init(self.ctx, C.byref(ip), C.c_void_p(_stream_ptr(stream))), "ymkh_init")
             torch.cuda.synchronize(self.device)
