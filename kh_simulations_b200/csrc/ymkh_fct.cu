@@ -64,13 +64,14 @@ __device__ __forceinline__ void beam_bar(int group, int nthreads) {
 
 // apply_fct_limiter (FCT_DeviceMath.cuh:108-125) with the products by
 // copysign(1, d0) written as flips of the sign bit: multiplying by -1 is an
-// exact negation, i.e. the same bits.
+// exact negation, i.e. the same bits.  The inner minima may differ from
+// fmin's only in the sign of a zero, which max_sel(+0, .) removes.
 __device__ __forceinline__ double flip_sign(double x, unsigned long long m) {
   return __longlong_as_double(__double_as_longlong(x) ^ m);
 }
 __device__ __forceinline__ double fct_limit_sel(double f, double dm1, double d0, double dp1) {
   const unsigned long long m = (unsigned long long)__double_as_longlong(d0) & 0x8000000000000000ull;
-  const double r = fmax(0.0, fmin(flip_sign(dm1, m), fmin(fabs(f), flip_sign(dp1, m))));
+  const double r = max_sel(0.0, min_sel(flip_sign(dm1, m), min_sel(fabs(f), flip_sign(dp1, m))));
   return flip_sign(r, m);
 }
 
@@ -261,11 +262,11 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
       // (YM_Fluid.cu:43-66, 71-80).
       double vz_own, ux_own, mu_if = 0.0, sx = 0.0;
       {
-        const double n0 = fmax(fl[FN * W + sp], 0.05);
+        const double n0 = max_sel(fl[FN * W + sp], 0.05);
         ux_own = fl[FPX * W + sp] / n0;
         vz_own = fl[FPZ * W + sp] / n0;
         if (t < TB - 1) {
-          const double n1 = fmax(fl[FN * W + sp + 1], 0.05);
+          const double n1 = max_sel(fl[FN * W + sp + 1], 0.05);
           const double u1 = fl[FPX * W + sp + 1] / n1;
           const double e = fct_eps(ux_own, u1, dtdx);
           double nu;
@@ -284,7 +285,7 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
             const int xg = x0 - 4 + sp;
             ps = (xg < 0 ? 0 : (xg >= nx ? nx - 1 : xg)) - (x0 - 4);
           }
-          const double vz = (ps == sp) ? vz_own : fl[FPZ * W + ps] / fmax(fl[FN * W + ps], 0.05);
+          const double vz = (ps == sp) ? vz_own : fl[FPZ * W + ps] / max_sel(fl[FN * W + ps], 0.05);
           double acc = 0.0;
 #pragma unroll
           for (int c = 0; c < 3; ++c) {

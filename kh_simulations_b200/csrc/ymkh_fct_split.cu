@@ -34,7 +34,7 @@ __device__ __forceinline__ double flip_sign2(double x, unsigned long long m) {
 }
 __device__ __forceinline__ double fct_limit_sel2(double f, double dm1, double d0, double dp1) {
   const unsigned long long m = (unsigned long long)__double_as_longlong(d0) & 0x8000000000000000ull;
-  const double r = fmax(0.0, fmin(flip_sign2(dm1, m), fmin(fabs(f), flip_sign2(dp1, m))));
+  const double r = max_sel(0.0, min_sel(flip_sign2(dm1, m), min_sel(fabs(f), flip_sign2(dp1, m))));
   return flip_sign2(r, m);
 }
 
@@ -85,9 +85,9 @@ __global__ void __launch_bounds__(2 * XT)
     double* const* fl = beam ? st.b : st.a;
 
     // ---- A: velocities at x and x+1, interface x+1/2, px source at x
-    const double n0 = fmax(fl[FN][row + xm], 0.05);
+    const double n0 = max_sel(fl[FN][row + xm], 0.05);
     const double u0 = fl[FPX][row + xm] / n0;
-    const double n1 = fmax(fl[FN][row + xp], 0.05);
+    const double n1 = max_sel(fl[FN][row + xp], 0.05);
     const double u1 = fl[FPX][row + xp] / n1;
     const double e = fct_eps(u0, u1, dtdx);
     double nu, mu;
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(2 * XT)
       const int xcm = xmap(wall ? (xc == 0 ? 0 : xc - 1) : xs - 1, nx, p.periodic_x);
       const int zm = (z == 0) ? nz - 1 : z - 1;
       const size_t rowm = (size_t)zm * nx;
-      const double vz = fl[FPZ][row + xc] / fmax(fl[FN][row + xc], 0.05);
+      const double vz = fl[FPZ][row + xc] / max_sel(fl[FN][row + xc], 0.05);
       double acc = 0.0;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(128)
       double Vx[3];
 #pragma unroll
       for (int j = 0; j < 3; ++j) Vx[j] = sl[ZV_X + j][lane];
-      const double n0 = fmax(sl[ZV_N][lane], 0.05);
+      const double n0 = max_sel(sl[ZV_N][lane], 0.05);
       const double vz = sl[ZV_PZ][lane] / n0;
       const double q1 = sl[ZV_Q + 0][lane], q2 = sl[ZV_Q + 1][lane], q3 = sl[ZV_Q + 2][lane];
       double S[3];
