@@ -25,14 +25,24 @@ namespace ymkh {
 
 namespace {
 
-// 62 output columns per strip: with 128 threads every phase is at most one
-// item per thread (63 velocity columns per beam = 126 items, 62 Ex columns
-// beside 63 Ez columns, Faraday's stores split over both halves), and the
+// 126 output columns per strip: with 256 threads every phase is at most one
+// item per thread (127 velocity columns per beam = 254 items, 126 Ex columns
+// beside 127 Ez columns, Faraday's stores split over both halves), and the
 // strip origin stays even, so staged rows start on 16-byte boundaries.
-constexpr int MX_TX = 62;        // output columns per strip
-constexpr int MX_NV = MX_TX + 1; // velocity / Ez columns (one right neighbour)
-constexpr int MX_NT = 128;       // threads per CTA: [0,64) Ex / By half, [64,128) Ez / store half
-constexpr int MX_NST = 3;        // stage ring depth: rows q-1, q in use, q+1 in flight
+// The shape can be set at build time (YMKH_MX_TX/NT/NST/MINB) for sweeps;
+// NT/2 >= TX + 1 keeps one item per thread per phase.  Measured at
+// 4096 x 8192 on B200 (Maxwell ms): 126/256/3 1.895, 62/128/3 1.934,
+// 30/64/3 2.207, 62/128/4 2.387.
+#ifndef YMKH_MX_TX
+#define YMKH_MX_TX 126
+#define YMKH_MX_NT 256
+#define YMKH_MX_NST 3
+#define YMKH_MX_MINB 2
+#endif
+constexpr int MX_TX = YMKH_MX_TX;    // output columns per strip
+constexpr int MX_NV = MX_TX + 1;     // velocity / Ez columns (one right neighbour)
+constexpr int MX_NT = YMKH_MX_NT;    // threads per CTA: [0,NT/2) Ex / By half, [NT/2,NT) Ez / store half
+constexpr int MX_NST = YMKH_MX_NST;  // stage ring depth: rows q-1, q in use, NST-2 rows in flight
 constexpr int MX_W = MX_TX + 4;  // stage row: position s <-> x = x0 - 2 + s (66: even)
 
 // stage offsets in rows of MX_W doubles (every array staged over the full row)
@@ -56,7 +66,7 @@ constexpr size_t maxwell_smem_bytes() {
          (size_t)8 * MX_NST + 16;
 }
 
-__global__ void __launch_bounds__(MX_NT, 4)
+__global__ void __launch_bounds__(MX_NT, YMKH_MX_MINB)
     maxwell_fused_kernel(const __grid_constant__ RunTable T) {
   constexpr int TX = MX_TX, NV = MX_NV, W = MX_W, NST = MX_NST, NT = MX_NT;
   static_assert(2 * NV <= NT && TX <= NT / 2 && NV <= NT / 2, "one item per thread per phase");
