@@ -151,7 +151,8 @@ int ymkh_set_current_buffer(ymkh_ctx* ctx, int which);
 
 /* Launch-shape controls used by the autotuner: steps per captured CUDA graph
  * (even, 0 = no graphs) and the FCT strip width (32/64/128) and z-segment
- * length.  No reference counterpart. */
+ * length (the unit of work that CTAs share out; each CTA runs a contiguous
+ * block of segments).  No reference counterpart. */
 int ymkh_set_graph_steps(ymkh_ctx* ctx, int nsteps_per_graph);
 int ymkh_set_fct_shape(ymkh_ctx* ctx, int strip_width, int segment_rows);
 int ymkh_get_fct_shape(ymkh_ctx* ctx, int* strip_width, int* segment_rows);

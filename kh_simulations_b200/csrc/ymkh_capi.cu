@@ -226,6 +226,8 @@ int pick_segment(int nz, int nstrips, int grid) {
   return best_seg;
 }
 
+constexpr int kFctSegment = 16;
+
 void choose_launch_shape(ymkh_ctx* c) {
   cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
   // 128-wide strips from NX = 1024 up: at 4096 x 8192 on B200 the step's FCT
@@ -233,8 +235,9 @@ void choose_launch_shape(ymkh_ctx* c) {
   c->fct_tx = c->nx >= 1024 ? 128 : (c->nx >= 128 ? 64 : 32);
   const int fct_per_sm = std::max(1, fct_ctas_per_sm(c->fct_tx));
   c->fct_grid = c->sms * fct_per_sm;
-  const int fstrips = fct_nstrips(c->nx, c->fct_tx);
-  c->fct_seg = pick_segment(c->nz, fstrips, c->fct_grid);
+  // segments are the FCT's unit of load balance: each CTA runs a contiguous
+  // block of them, a strip's part as one piece (ymkh_fct.cu)
+  c->fct_seg = std::min(c->nz, kFctSegment);
   const int mx_per_sm = std::max(1, maxwell_ctas_per_sm());
   c->mx_grid = c->sms * mx_per_sm;
   c->mx_seg = pick_segment(c->nz, maxwell_nstrips(c->nx), c->mx_grid);
@@ -849,7 +852,7 @@ int batch_build(ymkh_batch* b) {
     x0 += items_fx(d0, c->nz);
     z0 += items_fz(d0, c->nz);
     // finer segments than a lone run needs: items of many runs share the GPU
-    d0.fct_seg = d1.fct_seg = std::min(c->nz, 128);
+    d0.fct_seg = d1.fct_seg = std::min(c->nz, kFctSegment);
     d0.mx_seg = d1.mx_seg = std::min(c->nz, 128);
     d0.fct_item0 = d1.fct_item0 = f0;
     d0.mx_item0 = d1.mx_item0 = m0;

@@ -11,8 +11,8 @@
 // kernel_ym_precession, YM_Fluid.cu:32-108) are recomputed here from the
 // start-of-step state, which is what they are a function of.
 //
-// Layout: work items are (x-strip, z-segment) pairs, handed to persistent
-// CTAs round-robin.  A strip emits TB-6 columns; thread t of a beam owns
+// Layout: work items are (x-strip, z-segment) pairs; each persistent CTA
+// takes a contiguous block of them and runs each strip's part as one piece.  A strip emits TB-6 columns; thread t of a beam owns
 // stage position t+1 (shear index x0-3+t), and every x-sweep phase is at
 // most one position or interface per thread: interface quantities (eps, nu,
 // mu, low-order fluxes) are formed once per interface.  Threads [0,TB)
@@ -125,8 +125,16 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
   unsigned issued = 0, consumed = 0;  // rows issued / consumed by this CTA (all items)
   unsigned phase_bits = 0;            // per-stage mbarrier phase of the bulk path
 
-  for (int item = blockIdx.x; item < T.fct_items; item += gridDim.x) {
-    __syncthreads();  // previous item fully consumed
+  // Each CTA takes one contiguous block of the flattened items.  Within a
+  // run the items are strip-major (a strip's z-segments consecutive), and
+  // consecutive segments of one strip form one piece: the z pipeline warms
+  // up (6 rows) once per piece instead of once per segment, and the blocks
+  // differ by at most one segment.
+  const int per = (T.fct_items + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int i_beg = (int)blockIdx.x * per, i_end = min(T.fct_items, i_beg + per);
+  int next = i_beg;
+  for (int item = i_beg; item < i_end; item = next) {
+    __syncthreads();  // previous piece fully consumed
     if (tid == 0) s_run = find_run(T.runs, T.nruns, item, false);
     __syncthreads();
     load_desc(&rd, &T.runs[s_run]);
@@ -138,11 +146,14 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
     const double dt = p.dt;
     const double dtdx = p.dt / p.dx;
     const double dtdz = p.dt / p.dz;
+    const int nseg = (nz + rd.fct_seg - 1) / rd.fct_seg;
     const int local = item - rd.fct_item0;
-    const int strip = local % rd.fct_nstrips;
+    const int strip = local / nseg;
+    const int seg0 = local - strip * nseg;
+    next = min(i_end, rd.fct_item0 + (strip + 1) * nseg);  // past this piece's last segment
     const int x0 = strip * TO;
-    const int zs = (local / rd.fct_nstrips) * rd.fct_seg;
-    const int ze = min(nz, zs + rd.fct_seg);
+    const int zs = seg0 * rd.fct_seg;
+    const int ze = min(nz, (seg0 + (next - item)) * rd.fct_seg);
 
     if (!bulk)
       for (int i = tid; i < W; i += NT) xtab[i] = xmap(x0 - 4 + i, nx, p.periodic_x);
@@ -440,8 +451,8 @@ int fct_bulk_ok(const StepParams& p, int tb) { return (p.periodic_x && (p.nx % 2
 
 // The kernel reads start-of-step values across strip and segment halos while
 // other CTAs write theirs, so each run's fluid goes to its second buffer
-// (`out`); fields are only read.  grid_ctas persistent CTAs take the
-// flattened (run, strip, segment) items round-robin.
+// (`out`); fields are only read.  grid_ctas persistent CTAs take contiguous
+// blocks of the flattened (run, strip, segment) items.
 cudaError_t launch_fct_table(const RunTable& T, int tb, int grid_ctas, cudaStream_t s) {
   const int grid = std::max(1, std::min(T.fct_items, grid_ctas));
   switch (tb) {
