@@ -14,7 +14,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from cases import BITWISE, CASES, config
+from cases import BASE, BITWISE, CASES, config
 
 pytestmark = pytest.mark.gpu
 
@@ -271,3 +271,40 @@ def test_tiny_grids_vs_oracle(cuda, orc, nz, nx):
         s_gpu = run.state_numpy()
         run.close()
         assert np.array_equal(s_gpu, s_orc), (mode, np.abs(s_gpu - s_orc).max())
+
+
+STRIP_CASES = {
+    "bulk_512": "nz_override = 48\nnx_override = 512\nkz_keep_max = 15\n",
+    "warm_ragged_250": "nz_override = 40\nnx_override = 250\nwarm_T = 0.01\n",
+    "wall_300": "nz_override = 32\nnx_override = 300\n",
+    "filters_400": "nz_override = 64\nnx_override = 400\nsuppress_kz0 = 1\nhyp_diff = 5e-5\nkz_suppress_hi = 9\n",
+}
+
+
+@pytest.mark.parametrize("name", sorted(STRIP_CASES))
+def test_fct_strip_widths_identical(cuda, name):
+    """The fused FCT with 32-, 64- and 128-wide strips (short and long
+    segments) and the split form give the same state bit for bit after 3
+    steps: TMA rows and per-element rows (walls), warm_T rows, ragged
+    strips."""
+    from kh_simulations_b200 import _lib
+    from kh_simulations_b200.config import loads
+    from kh_simulations_b200.run import KHRun
+
+    text = BASE + STRIP_CASES[name]
+    if name.startswith("wall"):
+        text = text.replace("run_mode = 6", "run_mode = 0")
+    out = {}
+    for form in ((32, 8), (64, 16), (128, 16), (128, 5), "split"):
+        r = KHRun(loads(text, name))
+        r.init()
+        if form == "split":
+            _lib.check(r.lib.ymkh_set_fct_mode(r.ctx, _lib.FCT_SPLIT), "mode")
+        else:
+            _lib.check(r.lib.ymkh_set_fct_shape(r.ctx, *form), "shape")
+        r.step(3)
+        out[form] = r.state_numpy()
+        r.close()
+    ref = out[(64, 16)]
+    for form, st in out.items():
+        assert np.array_equal(st.view(np.uint64), ref.view(np.uint64)), form
