@@ -366,7 +366,7 @@ int post_stages(ymkh_ctx* c, const State& out, cudaStream_t s) {
 // One reference iteration from buffer c->cur into buffer 1 - c->cur.
 int step_once(ymkh_ctx* c, cudaStream_t s) {
   if (!c->desc_ok) { int rc = upload_desc(c); if (rc) return rc; }
-  RunTable T{c->ddesc + c->cur, 1, c->fct_items, c->mx_items, c->derr, c->fx_items, c->fz_items};
+  RunTable T{c->ddesc + c->cur, 1, c->fct_items, c->mx_items, c->derr, c->fx_items, c->fz_items, 1};
   mark(c, ST_FCT, s);
   {
     NvtxRange r("ymkh fct");
@@ -851,8 +851,8 @@ int batch_build(ymkh_batch* b) {
     d0.fz_item0 = d1.fz_item0 = z0;
     x0 += items_fx(d0, c->nz);
     z0 += items_fz(d0, c->nz);
-    // finer segments than a lone run needs: items of many runs share the GPU
-    d0.fct_seg = d1.fct_seg = std::min(c->nz, kFctSegment);
+    // batches take 128-row FCT segments round-robin (RunTable::fct_contig = 0)
+    d0.fct_seg = d1.fct_seg = std::min(c->nz, 128);
     d0.mx_seg = d1.mx_seg = std::min(c->nz, 128);
     d0.fct_item0 = d1.fct_item0 = f0;
     d0.mx_item0 = d1.mx_item0 = m0;
@@ -879,7 +879,7 @@ int batch_build(ymkh_batch* b) {
 int batch_step_once(ymkh_batch* b, cudaStream_t s) {
   const int n = (int)b->runs.size();
   if (!n) return 0;
-  RunTable T{b->ddesc + (size_t)b->parity * b->cap, n, b->fct_items, b->mx_items, b->derr, b->fx_items, b->fz_items};
+  RunTable T{b->ddesc + (size_t)b->parity * b->cap, n, b->fct_items, b->mx_items, b->derr, b->fx_items, b->fz_items, 0};
   if (b->fct_mode == YMKH_FCT_SPLIT)
     CK(launch_fct_split_table(T, b->fx_grid, b->fz_grid, s), "fct_x/fct_z kernels (batch)");
   else

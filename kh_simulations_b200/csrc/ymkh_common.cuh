@@ -288,6 +288,7 @@ struct RunTable {
   int fct_items, mx_items;
   unsigned* err;  // device error word of the bounded in-kernel waits
   int fx_items, fz_items;
+  int fct_contig;  // fused FCT: 1 = contiguous item blocks per CTA (lone run), 0 = round-robin (batches)
 };
 
 // Run owning item g of the split FCT's x pass (which = 0) or z pass (1).

@@ -11,8 +11,9 @@
 // kernel_ym_precession, YM_Fluid.cu:32-108) are recomputed here from the
 // start-of-step state, which is what they are a function of.
 //
-// Layout: work items are (x-strip, z-segment) pairs; each persistent CTA
-// takes a contiguous block of them and runs each strip's part as one piece.  A strip emits TB-6 columns; thread t of a beam owns
+// Layout: work items are (x-strip, z-segment) pairs; for a lone run each
+// persistent CTA takes a contiguous block of them and runs each strip's part
+// as one piece, for batches the CTAs take them round-robin.  A strip emits TB-6 columns; thread t of a beam owns
 // stage position t+1 (shear index x0-3+t), and every x-sweep phase is at
 // most one position or interface per thread: interface quantities (eps, nu,
 // mu, low-order fluxes) are formed once per interface.  Threads [0,TB)
@@ -125,13 +126,18 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
   unsigned issued = 0, consumed = 0;  // rows issued / consumed by this CTA (all items)
   unsigned phase_bits = 0;            // per-stage mbarrier phase of the bulk path
 
-  // Each CTA takes one contiguous block of the flattened items.  Within a
-  // run the items are strip-major (a strip's z-segments consecutive), and
-  // consecutive segments of one strip form one piece: the z pipeline warms
-  // up (6 rows) once per piece instead of once per segment, and the blocks
-  // differ by at most one segment.
-  const int per = (T.fct_items + (int)gridDim.x - 1) / (int)gridDim.x;
-  const int i_beg = (int)blockIdx.x * per, i_end = min(T.fct_items, i_beg + per);
+  // Lone run (T.fct_contig): each CTA takes one contiguous block of the
+  // flattened items.  Within a run the items are strip-major (a strip's
+  // z-segments consecutive), and consecutive segments of one strip form one
+  // piece: the z pipeline warms up (6 rows) once per piece instead of once
+  // per segment, and the blocks differ by at most one segment.  Batches
+  // take segment-major items round-robin, so the CTAs running at once work
+  // on neighbouring strips of the same rows and share halos through L2
+  // (3.5% faster on an uneven 64-run sweep).
+  const bool contig = T.fct_contig != 0;
+  const int per = contig ? (T.fct_items + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+  const int i_beg = contig ? (int)blockIdx.x * per : (int)blockIdx.x;
+  const int i_end = contig ? min(T.fct_items, i_beg + per) : T.fct_items;
   int next = i_beg;
   for (int item = i_beg; item < i_end; item = next) {
     __syncthreads();  // previous piece fully consumed
@@ -148,12 +154,20 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
     const double dtdz = p.dt / p.dz;
     const int nseg = (nz + rd.fct_seg - 1) / rd.fct_seg;
     const int local = item - rd.fct_item0;
-    const int strip = local / nseg;
-    const int seg0 = local - strip * nseg;
-    next = min(i_end, rd.fct_item0 + (strip + 1) * nseg);  // past this piece's last segment
+    int strip, zs, ze;
+    if (contig) {
+      strip = local / nseg;
+      const int seg0 = local - strip * nseg;
+      next = min(i_end, rd.fct_item0 + (strip + 1) * nseg);  // past this piece's last segment
+      zs = seg0 * rd.fct_seg;
+      ze = min(nz, (seg0 + (next - item)) * rd.fct_seg);
+    } else {
+      strip = local % rd.fct_nstrips;
+      zs = (local / rd.fct_nstrips) * rd.fct_seg;
+      ze = min(nz, zs + rd.fct_seg);
+      next = item + (int)gridDim.x;
+    }
     const int x0 = strip * TO;
-    const int zs = seg0 * rd.fct_seg;
-    const int ze = min(nz, (seg0 + (next - item)) * rd.fct_seg);
 
     if (!bulk)
       for (int i = tid; i < W; i += NT) xtab[i] = xmap(x0 - 4 + i, nx, p.periodic_x);
