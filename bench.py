@@ -233,6 +233,8 @@ def main() -> int:
     ap.add_argument("--filter-error-steps", type=int, default=0, help="steps of the TF32-vs-FP64 filter error leg")
     ap.add_argument("--filter-error-runs", type=int, default=2)
     ap.add_argument("--batched-runs", type=int, default=64, help="runs in the batched-vs-plain leg (0: skip)")
+    ap.add_argument("--batch-by-size", action="store_true",
+                    help="opt-in leg: batched against plain for identical runs of each size, 128x256 .. 1024x2048")
     ap.add_argument("--served-seconds", type=float, default=1.5, help="arrival window of the served leg (0: skip)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -332,6 +334,8 @@ def main() -> int:
         line["filter_error"] = filter_error(args, dev, args.filter_error_steps, args.filter_error_runs)
     if world == 1 and args.batched_runs > 0:
         line["batched"] = batched_rate(args, dev, args.batched_runs)
+    if world == 1 and args.batch_by_size:
+        line["batch_by_size"] = batch_by_size(dev)
     if world == 1 and args.served_seconds > 0:
         line["served"] = served_rate(args, dev, args.served_seconds)
     if rank == 0 and not args.no_cpu_baseline:
@@ -385,6 +389,53 @@ def _rel_l2_max(a, b) -> float:
     d = (a - b).reshape(a.shape[0], -1).norm(dim=1)
     n = b.reshape(b.shape[0], -1).norm(dim=1).clamp_min(1e-300)
     return float((d / n).max())
+
+
+def batch_by_size(dev) -> list:
+    """Batched against plain for identical runs of one size at a time (filter
+    off, CUDA events, one stream): where batching pays.  Sizes and counts:
+    64 x 128x256, 64 x 256x512, 32 x 512x1024, 8 x 1024x2048."""
+    import torch
+
+    from kh_simulations_b200.batch import KHBatch
+    from kh_simulations_b200.config import loads
+    from kh_simulations_b200.run import KHRun
+    from kh_simulations_b200.server import cfl_courant
+
+    out = []
+    for nz, nx, n, steps in [(128, 256, 64, 200), (256, 512, 64, 200), (512, 1024, 32, 100), (1024, 2048, 8, 40)]:
+        ini = (SWEEP_BASE + "V0 = 0.05\neps_override = 1.0\nperturb_amp = 0.1\nk_mode = 1\n"
+               f"nz_override = {nz}\nnx_override = {nx}\ncourant_override = {cfl_courant(nx, nz):.6f}\n")
+        runs = [KHRun(loads(ini, f"size{i}"), device=dev) for i in range(n)]
+        s = torch.cuda.Stream(device=dev)
+        for r in runs:
+            r.init(stream=s)
+            r.step(4, s)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for r in runs:
+            r.step(steps, s)
+        e1.record(s)
+        e1.synchronize()
+        plain = e0.elapsed_time(e1)
+        b = KHBatch(device=dev, graph_steps=4)
+        for r in runs:
+            b.add(r)
+        b.step(4, s)
+        torch.cuda.synchronize(dev)
+        e0.record(s)
+        b.step(steps, s)
+        e1.record(s)
+        e1.synchronize()
+        bat = e0.elapsed_time(e1)
+        cs = n * nz * nx * steps
+        out.append({"runs": n, "grid": f"{nz}x{nx}", "steps": steps, "plain_cell_steps_per_s": cs / plain * 1e3,
+                    "batched_cell_steps_per_s": cs / bat * 1e3, "batched_over_plain": plain / bat})
+        b.close()
+        for r in runs:
+            r.close()
+    return out
 
 
 def batched_rate(args, dev, nruns: int) -> dict:
