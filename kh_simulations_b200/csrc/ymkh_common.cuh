@@ -75,8 +75,7 @@ __device__ __forceinline__ double div_rn(double a, double b, double y) {
   return isinf(q) ? q : q1;
 }
 
-// FP64 min / max as one compare and a select (CUDA's fmin / fmax take about
-// 8.5 instructions each on sm_100).  min_sel(x, y) = fmin(x, y) and
+// FP64 min / max written as a compare and a select.  min_sel(x, y) = fmin(x, y) and
 // max_sel(x, y) = fmax(x, y) bit for bit, NaN operands included (a NaN
 // operand yields the other one), except for zeros of opposite sign, where
 // these return x:
