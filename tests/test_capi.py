@@ -65,3 +65,32 @@ int main(void){printf("%zu %zu %zu\n", sizeof(ymkh_grid), sizeof(ymkh_params), s
         subprocess.run(["gcc", "-I", str(ROOT / "include"), str(c), "-o", str(exe)], check=True)
         sizes = list(map(int, subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()))
     assert sizes == [C.sizeof(Grid), C.sizeof(Params), C.sizeof(InitParams)]
+
+
+def test_c_program_links_every_entry_point(built):
+    """A C program that takes the address of every entry point the header
+    declares compiles with gcc against include/ymkh.h and links against
+    libymkh.so: what a maintainer's shim beside main_ym.cu needs."""
+    import re
+    import tempfile
+
+    header = (ROOT / "include" / "ymkh.h").read_text()
+    names = sorted(set(re.findall(r"^\s*(?:int|long long)\s+(ymkh_\w+)\s*\(", header, flags=re.M)))
+    assert len(names) >= 30
+    src = "#include <stdio.h>\n#include \"ymkh.h\"\nint main(void){\n  void* fns[] = {\n"
+    src += ",\n".join(f"    (void*){n}" for n in names)
+    src += "\n  };\n  int n = 0;\n  for (unsigned i = 0; i < sizeof fns / sizeof fns[0]; ++i) n += fns[i] != 0;\n"
+    src += "  printf(\"%d\\n\", n);\n  return 0;\n}\n"
+    libdir = ROOT / "kh_simulations_b200"
+    cuda_lib = Path("/usr/local/cuda/lib64")
+    with tempfile.TemporaryDirectory() as td:
+        c = Path(td) / "shim.c"
+        c.write_text(src)
+        exe = Path(td) / "shim"
+        cmd = ["gcc", "-I", str(ROOT / "include"), str(c), "-o", str(exe), "-L", str(libdir), "-lymkh",
+               f"-Wl,-rpath,{libdir}", "-Wl,--allow-shlib-undefined"]
+        if cuda_lib.exists():
+            cmd += [f"-Wl,-rpath,{cuda_lib}"]
+        subprocess.run(cmd, check=True)
+        out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.strip()
+    assert int(out) == len(names)
