@@ -232,6 +232,8 @@ def main() -> int:
     ap.add_argument("--no-filter-leg", action="store_true", help="skip the FP64 vs TF32 band filter leg")
     ap.add_argument("--filter-error-steps", type=int, default=0, help="steps of the TF32-vs-FP64 filter error leg")
     ap.add_argument("--filter-error-runs", type=int, default=2)
+    ap.add_argument("--filter-error-control", action="store_true",
+                    help="the error leg as a control: FP64 filter against FP64 filter with Ez2 scaled by 1+2^-52 at the start")
     ap.add_argument("--batched-runs", type=int, default=64, help="runs in the batched-vs-plain leg (0: skip)")
     ap.add_argument("--batch-by-size", action="store_true",
                     help="opt-in leg: batched against plain for identical runs of each size, 128x256 .. 1024x2048")
@@ -331,7 +333,8 @@ def main() -> int:
     if world == 1 and not args.no_filter_leg:
         line["filter"] = filter_engines(args, dev)
     if world == 1 and args.filter_error_steps > 0:
-        line["filter_error"] = filter_error(args, dev, args.filter_error_steps, args.filter_error_runs)
+        line["filter_error"] = filter_error(args, dev, args.filter_error_steps, args.filter_error_runs,
+                                            control=args.filter_error_control)
     if world == 1 and args.batched_runs > 0:
         line["batched"] = batched_rate(args, dev, args.batched_runs)
     if world == 1 and args.batch_by_size:
@@ -587,7 +590,7 @@ def filter_engines(args, dev) -> dict:
     return out
 
 
-def filter_error(args, dev, steps: int, nruns: int) -> dict:
+def filter_error(args, dev, steps: int, nruns: int, control: bool = False) -> dict:
     """Error of the 3-pass TF32 filter against the FP64 filter, from the same
     initial state, on `nruns` runs at NZ 1024 x NX 2048 (seed 2,
     uneven-sweep parameter ranges, keep |k| <= NZ/3).  Both engines step in
@@ -595,7 +598,9 @@ def filter_error(args, dev, steps: int, nruns: int) -> dict:
     reference's halt rule (NaN/Inf or E/E0 above the threshold,
     ymgpu2d/main_ym.cu:467-474); the per-field relative L2 of the state and
     the relative error of the k_mode amplitude are taken at the last chunk
-    both completed."""
+    both completed.  With `control`, both runs use the FP64 filter and the
+    second starts with Ez2 scaled by 1 + 2^-52 (about one ulp): how far two
+    FP64 trajectories part from a rounding-level difference."""
     import math
 
     import numpy as np
@@ -616,9 +621,11 @@ def filter_error(args, dev, steps: int, nruns: int) -> dict:
     for cfg in split_precision_runs(2, nruns, SWEEP_BASE):
         runs = {}
         for eng in ("dft", "tf32x3"):
-            cfg.filter_engine = eng
+            cfg.filter_engine = "dft" if control else eng
             r = KHRun(cfg, device=dev)
             r.init()
+            if control and eng == "tf32x3":
+                r.state[STATE_NAMES.index("Ez2")] *= 1.0 + 2.0 ** -52
             r.E0 = r.energy()
             runs[eng] = r
         done = 0
@@ -648,7 +655,8 @@ def filter_error(args, dev, steps: int, nruns: int) -> dict:
         for r in runs.values():
             r.close()
         torch.cuda.empty_cache()
-    return {"workload": f"{nruns} runs at 1024x2048 (seed 2), keep |k| <= NZ/3, up to {steps} steps",
+    return {"workload": f"{nruns} runs at 1024x2048 (seed 2), keep |k| <= NZ/3, up to {steps} steps"
+                        + (", control: FP64 against FP64 with Ez2 scaled by 1+2^-52" if control else ""),
             "steps_reached": reached, "metric": "per-array rel-L2, divided by the largest norm in its group",
             "max_rel_l2_by_step": {str(c): {STATE_NAMES[i]: float(table[c][i]) for i in range(24)} for c in checkpoints},
             "max_rel_mode_amp_err_by_step": {str(c): amp[c] for c in checkpoints},
