@@ -233,7 +233,7 @@ def main() -> int:
     ap.add_argument("--filter-error-steps", type=int, default=0, help="steps of the TF32-vs-FP64 filter error leg")
     ap.add_argument("--filter-error-runs", type=int, default=2)
     ap.add_argument("--filter-error-control", action="store_true",
-                    help="the error leg as a control: FP64 filter against FP64 filter with Ez2 scaled by 1+2^-52 at the start")
+                    help="the error leg as a control: FP64 filter against FP64 filter with nA scaled by 1+2^-52 at the start")
     ap.add_argument("--batched-runs", type=int, default=64, help="runs in the batched-vs-plain leg (0: skip)")
     ap.add_argument("--batch-by-size", action="store_true",
                     help="opt-in leg: batched against plain for identical runs of each size, 128x256 .. 1024x2048")
@@ -599,8 +599,9 @@ def filter_error(args, dev, steps: int, nruns: int, control: bool = False) -> di
     ymgpu2d/main_ym.cu:467-474); the per-field relative L2 of the state and
     the relative error of the k_mode amplitude are taken at the last chunk
     both completed.  With `control`, both runs use the FP64 filter and the
-    second starts with Ez2 scaled by 1 + 2^-52 (about one ulp): how far two
-    FP64 trajectories part from a rounding-level difference."""
+    second starts with the beam-A density (about 1 everywhere) scaled by
+    1 + 2^-52, one ulp: how far two FP64 trajectories part from a
+    rounding-level difference."""
     import math
 
     import numpy as np
@@ -625,7 +626,7 @@ def filter_error(args, dev, steps: int, nruns: int, control: bool = False) -> di
             r = KHRun(cfg, device=dev)
             r.init()
             if control and eng == "tf32x3":
-                r.state[STATE_NAMES.index("Ez2")] *= 1.0 + 2.0 ** -52
+                r.state[STATE_NAMES.index("nA")] *= 1.0 + 2.0 ** -52
             r.E0 = r.energy()
             runs[eng] = r
         done = 0
@@ -656,7 +657,7 @@ def filter_error(args, dev, steps: int, nruns: int, control: bool = False) -> di
             r.close()
         torch.cuda.empty_cache()
     return {"workload": f"{nruns} runs at 1024x2048 (seed 2), keep |k| <= NZ/3, up to {steps} steps"
-                        + (", control: FP64 against FP64 with Ez2 scaled by 1+2^-52" if control else ""),
+                        + (", control: FP64 against FP64 with nA scaled by 1+2^-52" if control else ""),
             "steps_reached": reached, "metric": "per-array rel-L2, divided by the largest norm in its group",
             "max_rel_l2_by_step": {str(c): {STATE_NAMES[i]: float(table[c][i]) for i in range(24)} for c in checkpoints},
             "max_rel_mode_amp_err_by_step": {str(c): amp[c] for c in checkpoints},
