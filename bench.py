@@ -45,6 +45,7 @@ WORKLOADS = {
 PHYSICS = ("k_mode = 1\nalpha_YM = 1.0\nperturb_amp = 0.15\nrun_mode = 6\nV0 = 0.05\neps_override = 1.0\n"
            "lx_override = 20\ncourant_override = 0.4\n")
 BYTES_STEP = 376  # compulsory: read 24 FP64 arrays, write 23 (Az1 frozen)
+L2_BYTES = 126 << 20  # B200 L2
 BYTES_FCT = 288   # fct_fused_kernel: read 12 fluid + 12 field arrays, write 12 fluid
 BYTES_MAXWELL = 280  # maxwell_fused_kernel: read 24, write 11 (Az1 frozen)
 
@@ -178,12 +179,15 @@ def run_reference(args, world, rank, local):
     line = {"metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "filter": "none (reference cannot launch its band filter "
-                       "for NZ > 1024)"},
+            "config": {"workload": args.workload,
+                       "filter": ("keep |k| <= NZ/3" if WORKLOADS[args.workload][1] <= 1024
+                                  else "none (reference cannot launch its band filter for NZ > 1024)")},
             "cpu_baseline": {**cb, "value": value},
             "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     try:
         line["reference_cuda"] = ref_cuda_rate(args)
+        if args.ref_sweep_runs > 0:
+            line["reference_cuda_sweep"] = ref_sweep_rate(args, args.ref_sweep_runs)
     except Exception as e:  # the CPU arm stands on its own
         line["reference_cuda"] = {"unavailable": str(e)[:200]}
     print(json.dumps(line), flush=True)
@@ -216,6 +220,33 @@ def ref_cuda_rate(args) -> dict:
             "build": "reference sources unmodified, nvcc -O2 sm_100a (its stock flags)"}
 
 
+def ref_sweep_rate(args, nruns: int) -> dict:
+    """The reference's own kernels (stock build) over the uneven sweep of
+    the batched leg (seed 1, `nruns` runs), one run after another as its
+    campaign scripts run them: aggregate cell-steps/s over the timed steps."""
+    from kh_simulations_b200._lib import Grid
+    from kh_simulations_b200.config import derive, step_params
+    from kh_simulations_b200.run import init_params
+    from kh_simulations_b200.server import uneven_sweep
+    from oracle import REF_STOCK_LIB, RefHarness
+
+    if not REF_STOCK_LIB.exists():
+        raise RuntimeError("reference harness not built")
+    ms_total, cell_steps = 0.0, 0
+    for cfg in uneven_sweep(1, nruns, SWEEP_BASE):
+        d = derive(cfg)
+        ref = RefHarness(parity=False)
+        ref.create(Grid(d.nx, d.nz, d.dx, d.dz), step_params(cfg, d))
+        ip, _k = init_params(cfg, d)
+        ref.init(ip)
+        ref.step(max(1, args.warmup))
+        ms_total += ref.time_steps(args.steps)
+        cell_steps += d.nx * d.nz * args.steps
+        ref.destroy()
+    return {"workload": f"uneven sweep, {nruns} runs (seed 1), {args.steps} steps each, one run after another",
+            "value": cell_steps / (ms_total / 1e3), "unit": "cell-steps/s"}
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -235,6 +266,8 @@ def main() -> int:
     ap.add_argument("--filter-error-control", action="store_true",
                     help="the error leg as a control: FP64 filter against FP64 filter with nA scaled by 1+2^-52 at the start")
     ap.add_argument("--batched-runs", type=int, default=64, help="runs in the batched-vs-plain leg (0: skip)")
+    ap.add_argument("--ref-sweep-runs", type=int, default=0,
+                    help="--impl reference: also time the reference's kernels over the uneven sweep (0: skip)")
     ap.add_argument("--batch-by-size", action="store_true",
                     help="opt-in leg: batched against plain for identical runs of each size, 128x256 .. 1024x2048")
     ap.add_argument("--served-seconds", type=float, default=1.5, help="arrival window of the served leg (0: skip)")
@@ -315,7 +348,11 @@ def main() -> int:
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.workload, "nz_periodic": d.nz, "nx_shear": d.nx,
                        "filter": "keep |k| <= NZ/3" if d.bands else "none (as the reference at NZ > 1024)",
-                       "l2": "state 12.9 GB >> L2; no flush needed", "parallelism": f"replicas x{world}",
+                       "l2": (f"state {2 * 24 * 8 * cells / 1e9:.2f} GB > L2 (126 MB); no flush needed"
+                              if 2 * 24 * 8 * cells > L2_BYTES else
+                              f"state {2 * 24 * 8 * cells / 1e6:.0f} MB fits in L2 (126 MB): L2-resident, "
+                              "not a roofline workload"),
+                       "parallelism": f"replicas x{world}",
                        "graph_steps": 4},
             "roofline": roof,
             "step_roofline": {"bytes_per_cell_step": BYTES_STEP, "achieved": step_gbs, "peak": peak,
