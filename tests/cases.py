@@ -52,7 +52,8 @@ def config(name: str):
 
 # Cases stored as golden vectors from the reference's own kernels (32 x 32
 # grids keep the fixtures small).
-GOLDEN = ("keep_third", "ref_bands_kz0", "no_filter", "wall_mode0", "sponge_cut")
+GOLDEN = ("keep_third", "ref_bands_kz0", "no_filter", "wall_mode0", "sponge_cut", "warm", "dtanh_mode3",
+          "step_mode4", "cos_mode5", "circ_mode1", "emhd_mode2", "taper_by1eq", "unfrozen", "ragged")
 GOLDEN_STEPS = 2
 
 
