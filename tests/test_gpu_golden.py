@@ -42,3 +42,37 @@ def test_cuda_path_reproduces_reference_fixture(cuda, name):
     e = run.energy()
     assert abs(e - float(z["e1"])) <= 1e-13 * abs(float(z["e1"]))
     run.close()
+
+
+def test_config0_history_vs_reference_fixture(cuda):
+    """The config-0 run (NZ 256 x NX 512, keep |k| <= 85) against the
+    reference's stored history (tests/golden/make_history_fixture.py): the
+    energy every 10 steps within 1e-9, the k = 1 amplitude every 100 steps
+    within 1e-9, and the halt rule stopping both at the same check."""
+    from kh_simulations_b200.config import loads
+    from kh_simulations_b200.run import KHRun
+
+    z = np.load(GOLD / "history_config0.npz")
+    run = KHRun(loads(str(z["ini"]), "config0"))
+    run.init()
+    e0 = run.energy()
+    # compensated sum against the reference's sequential host sum over
+    # 131,072 cells: the latter's rounding is ~1e-13 relative here
+    assert abs(e0 - float(z["e0"])) <= 1e-12 * abs(float(z["e0"]))
+    ref_e, ref_a = z["energy_every_10"], z["mode1_every_100"]
+    energies, amps, halted_at = [], [], -1
+    for i in range(1, 1001):
+        run.step(10)
+        e = run.energy()
+        if not np.isfinite(e) or e / e0 > run.d.energy_thresh:
+            halted_at = 10 * i
+            break
+        energies.append(e)
+        if i % 10 == 0:
+            amps.append(run.mode_amp(1)[0])
+    assert halted_at == int(z["halted_at"])
+    assert len(energies) == len(ref_e) and len(ref_e) >= 100
+    dev = np.abs(np.array(energies) - ref_e) / np.abs(ref_e)
+    assert dev.max() < 1e-9, (dev.max(), int(dev.argmax()))
+    assert np.all(np.abs(np.array(amps) - ref_a) <= 1e-9 * np.abs(ref_a))
+    run.close()
