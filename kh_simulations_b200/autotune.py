@@ -2,10 +2,11 @@
 
 For a grid-size class (NZ and NX rounded to powers of two, band filter on or
 off) it times the fused FCT kernel for each candidate strip width (the tile
-shape: 32, 64 or 128 x-sweep positions per beam) and z-segment length
-(rows per work item, which sets how often the 3-row z halo is re-swept),
-then the split FCT form, then the number of steps per captured CUDA graph,
-and keeps the fastest.
+shape: 32, 64 or 128 x-sweep positions per beam) and z-segment length (the
+unit of work the persistent CTAs share out: each runs a contiguous block of
+segments, a strip's part as one piece with one 3-row halo warm-up), then the
+split FCT form, then the number of steps per captured CUDA graph, and keeps
+the fastest.
 Results are cached in a JSON table (``tuned.json`` beside this module, or
 the path in ``KH_TUNING_FILE``) that ``KHRun(tune=True)`` consults.
 
@@ -42,7 +43,7 @@ def lookup(nx: int, nz: int, filtered: bool):
 
 def candidates(nx: int, nz: int):
     tbs = [tb for tb in (32, 64, 128) if nx >= tb - 6]
-    segs = sorted({s for s in (32, 64, 128, 256, 512) if s <= max(32, nz)})
+    segs = sorted({s for s in (16, 32, 64, 128) if s <= max(16, nz)})
     return [(tb, s) for tb in tbs for s in segs]
 
 
