@@ -274,6 +274,9 @@ long long ymkh_launch_count(void);
  * YMKH_NOALLOC_MAX_CELLS cells; larger grids return YMKH_EINVAL.  The first
  * call on each device (that device current) looks up the array's address
  * (cudaGetSymbolAddress) and caches it: make it before any stream capture.
+ * The cache is per device and assumes the device's primary context (the
+ * runtime's): it is not valid under a caller's own driver-API context, nor
+ * across cudaDeviceReset. 
  * Calls that overlap on one device share the array and race: keep them on
  * one stream or one after another. */
 #define YMKH_NOALLOC_MAX_CELLS 134217728

@@ -49,10 +49,32 @@ def candidates(nx: int, nz: int):
 
 def tune(run, reps: int = 3, graph_candidates=(2, 4, 8), save: bool = True) -> dict:
     """Time the candidates on `run` (a KHRun, state initialised) and record
-    the best shape for its size class."""
+    the best shape for its size class.
+
+    Timing advances the state by many steps; the run's state is saved first
+    and put back afterwards, so the run continues its own trajectory from
+    where it was (same state, step count and energy reference)."""
     import torch
 
     lib = _lib.load()
+    torch.cuda.synchronize(run.device)
+    step_count = run.step_count
+    try:
+        saved = run.state.clone()
+    except torch.OutOfMemoryError:
+        saved = run.state.cpu()
+    try:
+        return _tune(run, lib, reps, graph_candidates, save)
+    finally:
+        torch.cuda.synchronize(run.device)
+        run.set_state(saved)
+        run.step_count = step_count
+        torch.cuda.synchronize(run.device)
+
+
+def _tune(run, lib, reps, graph_candidates, save) -> dict:
+    import torch
+
     stream = torch.cuda.Stream(device=run.device)
     out = (C.c_float * 8)()
     best = None

@@ -91,8 +91,10 @@ struct ymkh_ctx {
   bool aligned16 = false;   // every bound array 16-byte aligned: TMA bulk row copies allowed
   unsigned* derr = nullptr; // device error word of the bounded in-kernel waits
   RunDesc* ddesc = nullptr; // device run descriptors for start buffer 0 and 1
+  RunDesc hdesc[2]{};       // their host copy, uploaded in stream order by the next step call
   int fct_items = 0, mx_items = 0, fx_items = 0, fz_items = 0;
   bool desc_ok = false;
+  bool desc_pending = false; // hdesc not yet uploaded to ddesc
   int fct_mode = YMKH_FCT_FUSED;  // YMKH_FCT_FUSED or YMKH_FCT_SPLIT
   double* xscratch = nullptr;     // 12 x-swept fluid arrays of the split form
   int fz_seg = 128;
@@ -294,14 +296,36 @@ int upload_desc(ymkh_ctx* c) {
   if (!c->bound) return 0;
   if (!c->ddesc) CK(cudaMalloc(&c->ddesc, 2 * sizeof(RunDesc)), "cudaMalloc run descriptors");
   { int rc = ensure_xscratch(c); if (rc) return rc; }
-  RunDesc h[2] = {make_desc(c, 0, c->fct_tx, 0, 0), make_desc(c, 1, c->fct_tx, 0, 0)};
-  for (RunDesc& d : h) d.fx_item0 = d.fz_item0 = 0;
+  RunDesc* h = c->hdesc;
+  h[0] = make_desc(c, 0, c->fct_tx, 0, 0);
+  h[1] = make_desc(c, 1, c->fct_tx, 0, 0);
+  for (int i = 0; i < 2; ++i) h[i].fx_item0 = h[i].fz_item0 = 0;
   c->fct_items = items_fct(h[0], c->nz);
   c->mx_items = items_mx(h[0], c->nz);
   c->fx_items = items_fx(h[0], c->nz);
   c->fz_items = items_fz(h[0], c->nz);
-  CK(cudaMemcpy(c->ddesc, h, sizeof h, cudaMemcpyHostToDevice), "upload run descriptors");
+  c->desc_pending = true;  // uploaded by the next step call, on its stream
   c->desc_ok = true;
+  return 0;
+}
+
+// Table uploads are ordered on the stream of the step call that follows a
+// change, after the steps already queued there, so a table is never
+// rewritten under a kernel in flight on that stream.  Inside a stream
+// capture (where a pageable copy cannot be captured) the copy is synchronous.
+cudaError_t upload_table(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (s) cudaStreamIsCapturing(s, &cs);
+  if (cs != cudaStreamCaptureStatusNone) return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+  return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+}
+
+int flush_desc(ymkh_ctx* c, cudaStream_t s) {
+  if (!c->desc_ok) { int rc = upload_desc(c); if (rc) return rc; }
+  if (c->desc_pending) {
+    CK(upload_table(c->ddesc, c->hdesc, sizeof c->hdesc, s), "upload run descriptors");
+    c->desc_pending = false;
+  }
   return 0;
 }
 
@@ -365,7 +389,7 @@ int post_stages(ymkh_ctx* c, const State& out, cudaStream_t s) {
 
 // One reference iteration from buffer c->cur into buffer 1 - c->cur.
 int step_once(ymkh_ctx* c, cudaStream_t s) {
-  if (!c->desc_ok) { int rc = upload_desc(c); if (rc) return rc; }
+  { int rc = flush_desc(c, s); if (rc) return rc; }
   RunTable T{c->ddesc + c->cur, 1, c->fct_items, c->mx_items, c->derr, c->fx_items, c->fz_items, 1};
   mark(c, ST_FCT, s);
   {
@@ -448,17 +472,28 @@ int ymkh_create(const ymkh_grid* grid, const ymkh_params* params, ymkh_ctx** out
   if (grid->nx < 4 || grid->nz < 4) return set_err(YMKH_EINVAL, "grid too small (%d x %d)", grid->nx, grid->nz);
   if ((size_t)grid->nx * grid->nz > ((size_t)1 << 34)) return set_err(YMKH_EINVAL, "grid too large");
   ymkh_ctx* c = new ymkh_ctx();
-  CK(cudaGetDevice(&c->device), "cudaGetDevice");
+  // failures after this point release the context and what it holds
+#define CK_CREATE(call, what)                                                                 \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess) {                                                                  \
+      const int rc_ = set_err(YMKH_ECUDA, "%s: %s", what, cudaGetErrorString(e_));            \
+      ymkh_destroy(c);                                                                        \
+      return rc_;                                                                             \
+    }                                                                                         \
+  } while (0)
+  CK_CREATE(cudaGetDevice(&c->device), "cudaGetDevice");
   c->nx = grid->nx; c->nz = grid->nz; c->N = (size_t)grid->nx * grid->nz;
   int rc = setup_params(c, params);
   if (rc) { free_bands(c); delete c; return rc; }
-  CK(prepare_fct(32), "FCT kernel attributes");
-  CK(prepare_fct(64), "FCT kernel attributes");
-  CK(prepare_fct(128), "FCT kernel attributes");
-  CK(prepare_maxwell(), "Maxwell kernel attributes");
-  CK(prepare_fct_split(), "split FCT kernel attributes");
+  CK_CREATE(prepare_fct(32), "FCT kernel attributes");
+  CK_CREATE(prepare_fct(64), "FCT kernel attributes");
+  CK_CREATE(prepare_fct(128), "FCT kernel attributes");
+  CK_CREATE(prepare_maxwell(), "Maxwell kernel attributes");
+  CK_CREATE(prepare_fct_split(), "split FCT kernel attributes");
   choose_launch_shape(c);
-  CK(prepare_column(c->nz), "column kernel attributes");
+  CK_CREATE(prepare_column(c->nz), "column kernel attributes");
+#undef CK_CREATE
   const int np = energy_nparts(c->N);
   if (cudaMalloc(&c->epart, (size_t)2 * np * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->edev, 4 * sizeof(double)) != cudaSuccess ||
@@ -602,6 +637,7 @@ int ymkh_step(ymkh_ctx* c, int nsteps, void* stream) {
   if (nsteps < 0) return set_err(YMKH_EINVAL, "negative step count");
   NvtxRange range("ymkh_step");
   cudaStream_t s = (cudaStream_t)stream;
+  { int rc = flush_desc(c, s); if (rc) return rc; }  // before any capture of the steps
   int done = 0;
   const bool graphs = s != nullptr && c->graph_steps >= 2 && (c->graph_steps % 2) == 0;
   if (graphs) {
@@ -827,7 +863,7 @@ void batch_drop_graph(ymkh_batch* b) {
   if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; b->gstream = nullptr; }
 }
 
-int batch_build(ymkh_batch* b) {
+int batch_build(ymkh_batch* b, cudaStream_t s) {
   const int n = (int)b->runs.size();
   if (n > b->cap) {
     if (b->ddesc) cudaFree(b->ddesc);
@@ -866,9 +902,10 @@ int batch_build(ymkh_batch* b) {
   b->fx_items = x0;
   b->fz_items = z0;
   if (n) {
-    CK(cudaMemcpy(b->ddesc, h.data(), (size_t)n * sizeof(RunDesc), cudaMemcpyHostToDevice), "upload batch table");
-    CK(cudaMemcpy(b->ddesc + b->cap, h.data() + n, (size_t)n * sizeof(RunDesc), cudaMemcpyHostToDevice),
-       "upload batch table");
+    // in stream order after the steps already queued on s (a pageable
+    // source is staged before the call returns)
+    CK(upload_table(b->ddesc, h.data(), (size_t)n * sizeof(RunDesc), s), "upload batch table");
+    CK(upload_table(b->ddesc + b->cap, h.data() + n, (size_t)n * sizeof(RunDesc), s), "upload batch table");
   }
   b->parity = 0;
   b->dirty = false;
@@ -972,7 +1009,7 @@ int ymkh_batch_step(ymkh_batch* b, int nsteps, void* stream) {
   if (nsteps < 0) return set_err(YMKH_EINVAL, "negative step count");
   NvtxRange range("ymkh_batch_step");
   cudaStream_t s = (cudaStream_t)stream;
-  if (b->dirty) { int rc = batch_build(b); if (rc) return rc; }
+  if (b->dirty) { int rc = batch_build(b, s); if (rc) return rc; }
   int done = 0;
   const bool graphs = s != nullptr && b->graph_steps >= 2 && !b->runs.empty();
   if (graphs) {
@@ -1017,8 +1054,13 @@ int ymkh_batch_step(ymkh_batch* b, int nsteps, void* stream) {
     int rc = batch_step_once(b, s);
     if (rc) return rc;
   }
+  bool moved = false;
   for (ymkh_ctx* c : b->runs)
-    if (!c->dual && c->cur == 1) { int rc = copy_back(c, s); if (rc) return rc; }
+    if (!c->dual && c->cur == 1) { int rc = copy_back(c, s); if (rc) return rc; moved = true; }
+  // A member moved back to buffer 0 no longer matches the tables of the
+  // current parity (built for it starting in buffer 1): rebuild them from
+  // every member's current buffer before the next step.
+  if (moved) b->dirty = true;
   return 0;
 }
 

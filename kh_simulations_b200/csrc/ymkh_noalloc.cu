@@ -31,7 +31,11 @@
 // the scratch's device address with cudaGetSymbolAddress, checks the result
 // and caches it for that device; later calls reuse it.  The lookup can make
 // the runtime load this module onto the device, so make the first call on a
-// device before any stream capture begins.
+// device before any stream capture begins.  The cached address belongs to
+// the device's primary context, the one the CUDA runtime uses: a caller that
+// makes its own driver-API context current, or that calls cudaDeviceReset
+// after the first call, must not use this entry point afterwards (the cache
+// would hand out an address of another or a destroyed context).
 //
 // Concurrency: all calls on one device share the one scratch array.  Two
 // calls whose kernels may overlap (different streams, or different host

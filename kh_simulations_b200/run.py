@@ -106,6 +106,12 @@ class KHRun:
         """The current state buffer (a view; valid until the next step)."""
         return self.buf[self.current]
 
+    def fct_shape(self) -> tuple:
+        """(FCT strip width in threads per beam, z-segment rows) in use."""
+        tx, seg = C.c_int(), C.c_int()
+        check(self.lib.ymkh_get_fct_shape(self.ctx, C.byref(tx), C.byref(seg)), "ymkh_get_fct_shape")
+        return tx.value, seg.value
+
     def field(self, name: str) -> torch.Tensor:
         return self.state[STATE_NAMES.index(name)]
 

@@ -23,14 +23,17 @@ HERE = Path(__file__).resolve().parent
 ORACLE_LIB = HERE / "libymoracle.so"
 REF_PARITY_LIB = HERE / "_ref" / "libymref_parity.so"
 REF_STOCK_LIB = HERE / "_ref" / "libymref.so"
-REF_DIR = Path(os.environ.get("YMKH_REFERENCE_DIR", "/root/reference/ymgpu2d"))
+# The reference's ymgpu2d tree for the _ref targets: $YMKH_REFERENCE_DIR, else
+# the location the Makefile recipe names (absent on machines without it).
+REF_DIR = os.environ.get("YMKH_REFERENCE_DIR")
 
 NSTATE = 24
 
 
 def build(ref: bool = True) -> None:
-    targets = ["oracle"] + (["ref"] if ref and REF_DIR.exists() else [])
-    subprocess.run(["make", "-s", "-C", str(HERE), *targets, f"REF_DIR={REF_DIR}"], check=True)
+    targets = ["oracle"] + (["ref"] if ref else [])  # the recipe skips _ref when the tree is absent
+    subprocess.run(["make", "-s", "-C", str(HERE), *targets, *([f"REF_DIR={REF_DIR}"] if REF_DIR else [])],
+                   check=True)
 
 
 def _ptrs(state: np.ndarray):

@@ -2,7 +2,7 @@
 reference's own solver, ymgpu2d/analysis/ym_eigenmode.py, imported from the
 reference tree.
 
-    python tests/golden/make_eigen_fixtures.py
+    python tests/golden/make_eigen_fixtures.py <reference>/ymgpu2d
 
 For each case it runs the reference's solve_eigenmode and its mode choice
 and seed export steps (ym_eigenmode.py:336-440), and stores the chosen
@@ -20,7 +20,17 @@ from pathlib import Path
 
 import numpy as np
 
-REF = Path("/root/reference/ymgpu2d")
+def _ref_dir() -> Path:
+    """The reference's ymgpu2d tree: the first argument, else $YMKH_REFERENCE_DIR."""
+    import os
+
+    arg = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("YMKH_REFERENCE_DIR")
+    if not arg:
+        sys.exit(f"usage: python {Path(__file__).name} <reference ymgpu2d dir>  (or set YMKH_REFERENCE_DIR)")
+    return Path(arg)
+
+
+REF = _ref_dir() if __name__ == "__main__" else None
 OUT = Path(__file__).resolve().parent / "eigen_seeds.npz"
 
 # k_mode, alpha, V0, EPS, NX, LX, LZ, xi_sponge, xi_cut, shipped seed file (or "")

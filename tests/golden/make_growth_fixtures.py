@@ -1,9 +1,9 @@
 """Make tests/golden/growth_fits.json: amplitude histories and the growth
 rates that the reference's own fitters give on them.
 
-Run in a checkout that has the reference at /root/reference:
+Run with the reference's ymgpu2d tree at hand:
 
-    python tests/golden/make_growth_fixtures.py
+    python tests/golden/make_growth_fixtures.py <reference>/ymgpu2d
 
 Inputs:
 - the eleven runs of the reference's resolution study
@@ -29,7 +29,17 @@ from pathlib import Path
 
 import numpy as np
 
-REF = Path("/root/reference/ymgpu2d")
+def _ref_dir() -> Path:
+    """The reference's ymgpu2d tree: the first argument, else $YMKH_REFERENCE_DIR."""
+    import os
+
+    arg = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("YMKH_REFERENCE_DIR")
+    if not arg:
+        sys.exit(f"usage: python {Path(__file__).name} <reference ymgpu2d dir>  (or set YMKH_REFERENCE_DIR)")
+    return Path(arg)
+
+
+REF = _ref_dir() if __name__ == "__main__" else None
 OUT = Path(__file__).resolve().parent / "growth_fits.json"
 
 

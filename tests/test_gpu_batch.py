@@ -95,6 +95,46 @@ def test_continuous_batching_membership_changes(cuda):
         r.close()
 
 
+def test_batch_member_with_library_second_buffer(cuda):
+    """A member bound with ymkh_bind_state (the library owns its second
+    buffer, so an odd step count ends with a copy back to buffer 0) stays on
+    its own trajectory over batch calls of odd and even length: 5 then 6
+    batch steps equal 11 steps alone, for it and for a member bound with
+    both buffers."""
+    import ctypes as C
+
+    import torch
+
+    from kh_simulations_b200 import _lib
+    from kh_simulations_b200.batch import KHBatch
+    from kh_simulations_b200.run import KHRun
+
+    st = torch.cuda.Stream()
+    one = KHRun(_cfg(MIX[0][0]))
+    one.init()
+    torch.cuda.synchronize()
+    b0 = one.buf[0]
+    f = (C.c_void_p * 12)(*[b0[i].data_ptr() for i in range(12)])
+    a = (C.c_void_p * 6)(*[b0[12 + i].data_ptr() for i in range(6)])
+    bb = (C.c_void_p * 6)(*[b0[18 + i].data_ptr() for i in range(6)])
+    _lib.check(one.lib.ymkh_bind_state(one.ctx, f, a, bb), "ymkh_bind_state")
+    two = KHRun(_cfg(MIX[2][0]))
+    two.init()
+    b = KHBatch()
+    b.add(one)
+    b.add(two)
+    b.step(5, st)
+    assert one.current == 0
+    b.step(6, st)
+    st.synchronize()
+    b.check(st)
+    assert np.array_equal(one.state_numpy(), _alone(MIX[0][0], 11))
+    assert np.array_equal(two.state_numpy(), _alone(MIX[2][0], 11))
+    b.close()
+    one.close()
+    two.close()
+
+
 def test_server_mix_equals_sequential(cuda):
     from kh_simulations_b200.server import KHRequest, KHServer
 
@@ -120,6 +160,10 @@ def test_autotune_runs_and_keeps_results(cuda, tmp_path, monkeypatch):
     e = at.tune(r, reps=1, graph_candidates=(2, 4))
     assert e["fct_strip"] in (32, 64, 128) and e["graph_steps"] in (2, 4)
     assert at.lookup(r.d.nx, r.d.nz, True) == e
+    # tuning put the run back where it was: it continues its own trajectory
+    assert r.step_count == 0
+    r.step(4)
+    assert np.array_equal(r.state_numpy(), _alone(MIX[2][0], 4))
     s_tuned = KHRun(_cfg(MIX[2][0]), tune=True)
     s_tuned.init()
     s_tuned.step(4)

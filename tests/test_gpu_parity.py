@@ -15,6 +15,7 @@ import numpy as np
 import pytest
 
 from cases import BASE, BITWISE, CASES, config
+from parity_report import record
 
 pytestmark = pytest.mark.gpu
 
@@ -117,7 +118,8 @@ def test_step_vs_reference_and_oracle(cuda, ref, orc, name):
     else:
         # band filter: the oracle follows the reference's summation tree
         assert np.array_equal(s_orc, s_ref), f"oracle vs reference: max {np.abs(s_orc - s_ref).max()}"
-        assert rel_l2(s_gpu, s_ref).max() < FILTER_TOL, rel_l2(s_gpu, s_ref)
+        rep = record(name, nsteps, s_gpu, s_ref, "band filter, 32 x 48")
+        assert rel_l2(s_gpu, s_ref).max() < FILTER_TOL, rep
     assert np.isfinite(s_gpu).all()
     run.close()
 
