@@ -11,8 +11,8 @@ Filter: the reference's band-filter kernels launch one thread per z cell
 and cannot launch for NZ > 1024 (ymgpu2d/main_ym.cu:396, YM_Physics.cu:349),
 so the reference's own step at this size performs no filtering; the default
 ``--filter ref`` reproduces that.  ``--filter keep`` subtracts modes above
-NZ/3 every step with the dense FP64 contraction (reported under
-``filter_keep`` when ``--with-filter-line`` is given).
+NZ/3 every step with the dense FP64 contraction; the ``filter_keep``
+field times config 1 as stated (filter on) with both filter engines.
 
 One step = one iteration of the reference loop over the whole grid.  The
 state (12.9 GB for two buffers) is far larger than L2 (126 MB), so no flush
@@ -162,6 +162,64 @@ def cpu_oracle_rate(workload: str, steps: int, threads: int | None = None, min_s
                       f"{nx * nz} cells, no band filter, {dt:.2f} s"}
 
 
+CONFIG0 = PHYSICS + "nz_override = 256\nnx_override = 512\nkz_keep_max = 85\n"
+
+
+def cpu_baselines(repeats: int = 5) -> dict:
+    """The FP64 OpenMP oracle on all host cores, median of `repeats` timed
+    runs each: config 0 (256 x 512, keep |k| <= 85, the band filter with the
+    FP32 twiddle table) for 5 steps, and the first 8 runs of the uneven sweep
+    (seed 1, config 2's distributions) for 1 step each, as an aggregate."""
+    import numpy as np
+
+    from kh_simulations_b200._lib import Grid
+    from kh_simulations_b200.config import derive, loads, step_params
+    from kh_simulations_b200.server import uneven_sweep
+    from oracle import Oracle
+
+    orc = Oracle()
+
+    def initial(d):
+        st = np.zeros((24, d.nz, d.nx))
+        st[12] = st[18] = 1.0
+        st[15], st[21] = 1.0, -1.0
+        xi = (np.arange(d.nx) * d.dx - d.nx * d.dx * 0.5) / d.eps
+        st[14] = d.V0 * np.tanh(xi)[None, :]
+        st[20] = -st[14]
+        st[10] = 1e-3 * np.cos(2 * np.pi * np.arange(d.nz) / d.nz)[:, None]
+        return st
+
+    def setup(cfg):
+        d = derive(cfg)
+        tw = None
+        if d.bands:
+            tw = orc.twiddles(d.nz, 0, max(hi for _, hi in d.bands))
+        return d, Grid(d.nx, d.nz, d.dx, d.dz), step_params(cfg, d), initial(d), tw
+
+    out = {"cores": orc.threads(), "kind": "port", "repeats": repeats, "statistic": "median"}
+    d, g, p, st, tw = setup(loads(CONFIG0))
+    orc.step(g, p, st, 1, twiddles=tw)
+    rates = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        orc.step(g, p, st, 5, twiddles=tw)
+        rates.append(d.nx * d.nz * 5 / (time.perf_counter() - t0))
+    out["config0"] = {"value": statistics.median(rates), "unit": "cell-steps/s",
+                      "sample": "256x512 (NZ x NX), keep |k| <= 85 (band filter on), 5 steps per run"}
+    runs = [setup(c) for c in uneven_sweep(1, 8, SWEEP_BASE)]
+    for d, g, p, st, tw in runs:
+        orc.step(g, p, st, 1, twiddles=tw)
+    rates = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        for d, g, p, st, tw in runs:
+            orc.step(g, p, st, 1, twiddles=tw)
+        rates.append(sum(d.nx * d.nz for d, *_ in runs) / (time.perf_counter() - t0))
+    out["config2_subset"] = {"value": statistics.median(rates), "unit": "cell-steps/s",
+                             "sample": "first 8 runs of the uneven sweep (seed 1), 1 step each, aggregate"}
+    return out
+
+
 def run_reference(args, world, rank, local):
     """Reference arm: the reference's own step on the host cores (it has no
     CPU implementation, so this is the FP64 OpenMP port), plus the
@@ -186,17 +244,22 @@ def run_reference(args, world, rank, local):
             "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     try:
         line["reference_cuda"] = ref_cuda_rate(args)
+        line["reference_cuda_config0"] = ref_cuda_rate(args, CONFIG0, steps=200,
+                                                       what="config 0: 256x512, keep |k| <= 85")
         if args.ref_sweep_runs > 0:
             line["reference_cuda_sweep"] = ref_sweep_rate(args, args.ref_sweep_runs)
     except Exception as e:  # the CPU arm stands on its own
         line["reference_cuda"] = {"unavailable": str(e)[:200]}
+    if not args.no_cpu_baseline:
+        line["cpu_baselines"] = cpu_baselines()
     print(json.dumps(line), flush=True)
     return 0
 
 
-def ref_cuda_rate(args) -> dict:
+def ref_cuda_rate(args, ini: str | None = None, steps: int | None = None, what: str | None = None) -> dict:
     """The reference's own kernels (oracle/_ref/libymref.so, its stock
-    flags) through its own stage sequence, timed with CUDA events."""
+    flags) through its own stage sequence, timed with CUDA events, on the
+    workload (or on `ini`)."""
     import torch
 
     from kh_simulations_b200._lib import Grid
@@ -206,18 +269,22 @@ def ref_cuda_rate(args) -> dict:
 
     if not torch.cuda.is_available() or not REF_STOCK_LIB.exists():
         raise RuntimeError("no GPU or reference harness not built")
-    cfg = loads(ini_for(args.workload, "ref"))
+    cfg = loads(ini if ini else ini_for(args.workload, "ref"))
+    steps = steps or args.steps
     d = derive(cfg)
     ref = RefHarness(parity=False)
     ref.create(Grid(d.nx, d.nz, d.dx, d.dz), step_params(cfg, d))
     ip, _k = init_params(cfg, d)
     ref.init(ip)
     ref.step(max(1, args.warmup))
-    ms = ref.time_steps(args.steps)
+    ms = ref.time_steps(steps)
     ref.destroy()
     cells = d.nx * d.nz
-    return {"value": cells * args.steps / (ms / 1e3), "unit": "cell-steps/s", "ms_per_step": ms / args.steps,
-            "build": "reference sources unmodified, nvcc -O2 sm_100a (its stock flags)"}
+    out = {"value": cells * steps / (ms / 1e3), "unit": "cell-steps/s", "ms_per_step": ms / steps,
+           "build": "reference sources unmodified, nvcc -O2 sm_100a (its stock flags)"}
+    if what:
+        out["workload"] = what
+    return out
 
 
 def ref_sweep_rate(args, nruns: int) -> dict:
@@ -257,7 +324,8 @@ def main() -> int:
     ap.add_argument("--filter", choices=["ref", "keep"], default="ref")
     ap.add_argument("--filter-engine", choices=["dft", "tf32x3"], default="dft",
                     help="band filter of the main run: FP64 sums or 3-pass TF32 on the tensor cores")
-    ap.add_argument("--with-filter-line", action="store_true")
+    ap.add_argument("--no-filter-keep", action="store_true",
+                    help="skip the config-1-as-stated leg (filter on at the workload size, both engines)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-filter-leg", action="store_true", help="skip the FP64 vs TF32 band filter leg")
@@ -266,11 +334,20 @@ def main() -> int:
     ap.add_argument("--filter-error-control", action="store_true",
                     help="the error leg as a control: FP64 filter against FP64 filter with nA scaled by 1+2^-52 at the start")
     ap.add_argument("--batched-runs", type=int, default=64, help="runs in the batched-vs-plain leg (0: skip)")
-    ap.add_argument("--ref-sweep-runs", type=int, default=0,
+    ap.add_argument("--ref-sweep-runs", type=int, default=64,
                     help="--impl reference: also time the reference's kernels over the uneven sweep (0: skip)")
     ap.add_argument("--batch-by-size", action="store_true",
                     help="opt-in leg: batched against plain for identical runs of each size, 128x256 .. 1024x2048")
-    ap.add_argument("--served-seconds", type=float, default=1.5, help="arrival window of the served leg (0: skip)")
+    ap.add_argument("--served-seconds", type=float, default=60.0, help="arrival window of the served leg (0: skip)")
+    ap.add_argument("--served-drain", type=float, default=60.0,
+                    help="served leg: each pass stops this long after the last arrival at the latest "
+                         "(a safety bound; the default mix drains well before it)")
+    ap.add_argument("--served-step-scale", type=int, default=200,
+                    help="served leg: config 4's 2000..20000 steps per request divided by this")
+    ap.add_argument("--served-fp64-seconds", type=float, default=6.0,
+                    help="arrival window of the served leg with the FP64 filter (0: skip)")
+    ap.add_argument("--served-check", type=int, default=6,
+                    help="requests in the served tolerance check against plain FP64 runs (0: skip)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -365,7 +442,7 @@ def main() -> int:
     del run
     torch.cuda.empty_cache()
 
-    if args.with_filter_line and args.filter == "ref" and d.nz > 1024:
+    if world == 1 and not args.no_filter_keep and args.filter == "ref" and d.nz > 1024:
         line["filter_keep"] = filter_keep_rate(args, dev)
     if world == 1 and not args.no_filter_leg:
         line["filter"] = filter_engines(args, dev)
@@ -378,12 +455,42 @@ def main() -> int:
         line["batch_by_size"] = batch_by_size(dev)
     if world == 1 and args.served_seconds > 0:
         line["served"] = served_rate(args, dev, args.served_seconds)
+    if world == 1:
+        line["config0"] = config0_rate(dev)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_oracle_rate(args.workload, 1, min_seconds=10.0)
+        line["cpu_baselines"] = cpu_baselines()
     if rank == 0:
         print(json.dumps(line), flush=True)
     replicas.finish(rk)
     return 0
+
+
+def config0_rate(dev, steps: int = 1000) -> dict:
+    """Config 0 (256 x 512, keep |k| <= 85, 1000 steps): device time of the
+    plain single-run step with CUDA events (4-step graphs).  The state
+    (100 MB for two buffers) fits in L2: a launch-and-latency figure, not a
+    roofline one."""
+    import torch
+
+    from kh_simulations_b200.config import loads
+    from kh_simulations_b200.run import KHRun
+
+    run = KHRun(loads(CONFIG0), device=dev)
+    run.init()
+    stream = torch.cuda.Stream(device=dev)
+    run.step(8, stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    run.step(steps, stream)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    cells = run.d.nx * run.d.nz
+    run.close()
+    return {"workload": "config 0: 256x512, keep |k| <= 85", "steps": steps, "ms_per_step": ms / steps,
+            "value": cells * steps / (ms / 1e3), "unit": "cell-steps/s"}
 
 
 def e2e_rate(run, args, stream, rk) -> dict:
@@ -539,51 +646,138 @@ def batched_rate(args, dev, nruns: int) -> dict:
             "max_rel_l2_batched_vs_plain": dev_max, "unit": "cell-steps/s", "timing": "CUDA events, one stream"}
 
 
-def served_rate(args, dev, seconds: float) -> dict:
-    """Served request mix scaled to the bench's time budget: Poisson arrivals
-    at 20 runs/s for `seconds` s (seed 3), cells log-uniform in
-    [128*256, 2048*4096], steps uniform in [200, 2000] (the full mix has
-    2000..20000), 150 GB admission budget, split-precision filtering on
-    (modes above NZ/3 subtracted with the 3-pass TF32 tensor-core filter).
-    The full mix offers about 80x what one B200 steps per second; at a tenth
-    of the steps the scaled mix still offers several times its capacity, so
-    both passes run saturated and their throughputs compare capacities.
-    Continuous batching (KHServer.serve) against the same requests one by
-    one through the plain step (serve_sequential); p50/p99 run latency from
-    arrival to completion; per-request final energies of the two passes are
-    compared."""
-    import math
-
+def _served_pass(dev, seconds, drain, step_scale, engine, large_cells):
+    """One served and one sequential pass over the same seeded mix (seed 3):
+    Poisson arrivals at 20 runs/s for `seconds` s, cells log-uniform in
+    [128*256, 2048*4096], steps uniform in [2000, 20000] / step_scale, modes
+    above NZ/3 subtracted with `engine`, 150 GB admission budget; each pass
+    stops `drain` s after the last arrival at the latest."""
     from kh_simulations_b200.server import KHServer, poisson_mix
 
     def mix():
-        return poisson_mix(3, 20.0, seconds, 128 * 256, 2048 * 4096, 200, 2000, SWEEP_BASE, keep_third=True,
-                           filter_engine="tf32x3")
+        return poisson_mix(3, 20.0, seconds, 128 * 256, 2048 * 4096, max(1, 2000 // step_scale),
+                           max(2, 20000 // step_scale), SWEEP_BASE, keep_third=True, filter_engine=engine)
 
-    srv = KHServer(150 << 30, device=dev, chunk=50)
-    served = srv.serve(mix())
-    seq = srv.serve_sequential(mix())
-    ea = {r.rid: r.energy for r in served.requests}
-    de = max((abs(r.energy - ea[r.rid]) / abs(r.energy) for r in seq.requests
-              if math.isfinite(r.energy) and r.energy != 0), default=0.0)
+    srv = KHServer(150 << 30, device=dev, chunk=50, large_cells=large_cells)
+    served = srv.serve(mix(), deadline=seconds + drain)
+    seq = srv.serve_sequential(mix(), deadline=seconds + drain)
     a, b = served.summary(), seq.summary()
-    keys = ("requests", "completed", "halted", "makespan_s", "cell_steps_per_s", "p50_latency_s", "p99_latency_s")
-    return {"workload": f"Poisson 20/s for {seconds:g} s (seed 3), 128x256..2048x4096 cells, 200..2000 steps, "
-                        "150 GB budget, keep |k| <= NZ/3 with the TF32 tensor-core filter",
-            "served": {k: a[k] for k in keys}, "sequential": {k: b[k] for k in keys},
+    keys = ("requests", "completed", "unfinished", "halted", "makespan_s", "cell_steps", "cell_steps_per_s",
+            "p50_latency_s", "p99_latency_s")
+    # measured Amdahl bound: service time of the sequential pass split into
+    # runs below / at or above large_cells; batching can at best remove the
+    # former, since a large run fills the GPU alone
+    t_small = sum(r.finished - r.admitted for r in seq.requests
+                  if r.status in ("done", "halted") and r.cells < large_cells)
+    t_large = sum(r.finished - r.admitted for r in seq.requests
+                  if r.status in ("done", "halted") and r.cells >= large_cells)
+    w = [(r.cells * r.steps, r.cells < large_cells) for r in mix()]
+    return {"engine": engine, "served": {k: a[k] for k in keys}, "sequential": {k: b[k] for k in keys},
             "served_over_sequential": a["cell_steps_per_s"] / b["cell_steps_per_s"] if b["cell_steps_per_s"] else None,
-            "max_rel_energy_diff": de, "unit": "cell-steps/s", "latency_clock": "host wall clock (arrival to completion)"}
+            "p50_served_over_sequential": a["p50_latency_s"] / b["p50_latency_s"] if b["p50_latency_s"] else None,
+            "small_runs_share_of_cell_steps": sum(x for x, sm in w if sm) / max(1, sum(x for x, _ in w)),
+            "small_runs_share_of_sequential_time": t_small / max(1e-9, t_small + t_large),
+            "amdahl_bound_served_over_sequential": (t_small + t_large) / t_large if t_large > 0 else None}
+
+
+def _served_tolerance(dev, step_scale, nreq, large_cells):
+    """Final states of the first `nreq` requests of the mix (seed 3, runs up
+    to 1024 x 2048), served with the FP64 filter and with the TF32 filter,
+    against the same requests run one by one plainly with the FP64 filter:
+    the largest per-field relative L2 over requests and arrays, raw (over
+    the field's own norm) and over the largest norm in the field's group."""
+    import numpy as np
+
+    from kh_simulations_b200.server import KHServer, poisson_mix
+
+    groups = [range(0, 6), range(6, 9), range(9, 12), [12], [13, 14], range(15, 18), [18], [19, 20], range(21, 24)]
+
+    def reqs(engine):
+        out = [r for r in poisson_mix(3, 20.0, 30.0, 128 * 256, 2048 * 4096, max(1, 2000 // step_scale),
+                                      max(2, 20000 // step_scale), SWEEP_BASE, keep_third=True,
+                                      filter_engine=engine) if r.cells <= 1024 * 2048][:nreq]
+        for r in out:
+            r.arrival = 0.0
+        return out
+
+    srv = KHServer(150 << 30, device=dev, chunk=50, keep_state=True, large_cells=large_cells)
+    plain = reqs("dft")
+    srv.serve_sequential(plain)
+    res = {}
+    for engine in ("dft", "tf32x3"):
+        rs = reqs(engine)
+        srv.serve(rs)
+        raw = grp = 0.0
+        for a, b in zip(rs, plain):
+            if a.status != "done" or b.status != "done":
+                continue
+            num = np.sqrt(((a.state - b.state) ** 2).reshape(24, -1).sum(1))
+            nrm = np.sqrt((b.state ** 2).reshape(24, -1).sum(1))
+            raw = max(raw, float(np.max(np.where(nrm > 0, num / np.where(nrm > 0, nrm, 1), num))))
+            for g in groups:
+                g = list(g)
+                grp = max(grp, float(num[g].max() / max(nrm[g].max(), 1e-300)))
+        res[engine] = {"max_rel_l2_vs_fp64_plain_raw": raw, "max_rel_l2_vs_fp64_plain_group": grp,
+                       "within_1e-10": raw <= 1e-10,
+                       "requests": [f"{derive_grid(r)} x {r.steps} steps ({r.status})" for r in rs]}
+    return res
+
+
+def derive_grid(req) -> str:
+    from kh_simulations_b200.config import derive
+
+    d = derive(req.cfg)
+    return f"{d.nz}x{d.nx}"
+
+
+def served_rate(args, dev, seconds: float) -> dict:
+    """Served request mix with config 4's distributions (Poisson 20 runs/s,
+    cells log-uniform in [128*256, 2048*4096], kz = 0 suppressed in every
+    other request, modes above NZ/3 subtracted) over a `seconds`-long arrival
+    window, steps scaled down by --served-step-scale, each pass bounded to
+    --served-drain s after the last arrival (unfinished runs count their
+    steps and their latency is censored there).  The full mix offers about
+    200 times what one B200 steps per second; the scaled one still offers
+    more than its capacity, so both passes run saturated and their
+    throughputs compare capacities.  Continuous batching (KHServer.serve:
+    runs of 2^20 cells and more stepped alone in arrival order on their own
+    stream, the smaller ones batched beside them) against the same requests
+    one by one through the plain step (serve_sequential).  The TF32 filter
+    (config 4's split precision) is the headline; the FP64 filter pass keeps
+    the 1e-10 bar; a tolerance leg compares final states of both served
+    forms with the plain FP64 runs."""
+    large = 1 << 20
+    out = {"workload": f"Poisson 20/s for {seconds:g} s (seed 3), 128x256..2048x4096 cells, "
+                       f"{2000 // args.served_step_scale}..{20000 // args.served_step_scale} steps "
+                       f"(config 4's 2000..20000 / {args.served_step_scale}), 150 GB budget, keep |k| <= NZ/3, "
+                       f"passes bounded at {args.served_drain:g} s after the last arrival",
+           "large_cells": large, "unit": "cell-steps/s",
+           "latency_clock": "host wall clock (arrival to completion; unfinished runs censored at the bound)"}
+    out["tf32x3"] = _served_pass(dev, seconds, args.served_drain, args.served_step_scale, "tf32x3", large)
+    if args.served_fp64_seconds > 0:
+        out["dft"] = _served_pass(dev, args.served_fp64_seconds, args.served_drain, args.served_step_scale, "dft",
+                                  large)
+    if args.served_check > 0:
+        tol = _served_tolerance(dev, args.served_step_scale, args.served_check, large)
+        out["tolerance"] = tol
+        out["tf32x3"]["max_rel_l2_vs_fp64_plain"] = tol["tf32x3"]["max_rel_l2_vs_fp64_plain_raw"]
+        out["tf32x3"]["within_metric_1e-10"] = tol["tf32x3"]["within_1e-10"]
+        if "dft" in out:
+            out["dft"]["max_rel_l2_vs_fp64_plain"] = tol["dft"]["max_rel_l2_vs_fp64_plain_raw"]
+            out["dft"]["within_metric_1e-10"] = tol["dft"]["within_1e-10"]
+    return out
 
 
 def measured_tf32_peak() -> tuple:
     """TF32 dense tensor rate: half the measured bf16 dense burst rate (the
-    B200's TF32 rate is half its bf16 rate); nominal 1.1 PFLOP/s otherwise."""
+    B200's TF32 rate is half its bf16 rate); without MEASURED_PEAKS.json,
+    half of the profiling recipe's fallback bf16 figure (1.59 PFLOP/s)."""
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
         if "bf16_tflops" in d:
             return float(d["bf16_tflops"]) / 2.0, "half of measured bf16 dense"
-    return 1100.0, "nominal"
+    return 1590.0 / 2.0, "half of fallback bf16 dense (1.59 PFLOP/s)"
 
 
 def filter_engines(args, dev) -> dict:
@@ -702,28 +896,72 @@ def filter_error(args, dev, steps: int, nruns: int, control: bool = False) -> di
 
 
 def filter_keep_rate(args, dev) -> dict:
+    """The workload as config 1 states it, filter on: modes above NZ/3
+    subtracted every step (at NZ = 4096, modes 1366..2048 of 21 arrays), with
+    the FP64 DFT engine and with the 3-pass TF32 tensor-core engine.  For
+    each: step time (CUDA events over plain steps), cell-steps/s and the band
+    stage's share; for TF32, the band stage's tensor roofline (algorithmic
+    flops of the two contractions per array over its device time, and 3x that
+    executed, against half the measured bf16 dense rate) and its error
+    against the FP64 engine after one step from the same state (per-field
+    relative L2, raw and over the largest norm in the field's group)."""
+    import numpy as np
     import torch
 
+    from kh_simulations_b200 import _lib
     from kh_simulations_b200.config import loads
     from kh_simulations_b200.run import KHRun
 
-    cfg = loads(ini_for(args.workload, "keep"))
-    run = KHRun(cfg, device=dev)
-    run.init()
-    stream = torch.cuda.Stream(device=dev)
-    run.step(2, stream)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    n = 2
-    e0.record(stream)
-    run.step(n, stream)
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    ms = e0.elapsed_time(e1) / n
-    cells = run.d.nx * run.d.nz
-    run.close()
-    return {"value": cells / (ms / 1e3), "unit": "cell-steps/s", "ms_per_step": ms,
-            "bands": run.d.bands}
+    lib = _lib.load()
+    out = {"workload": f"{args.workload}, keep |k| <= NZ/3 (config 1 as stated), 21 filtered arrays"}
+    states = {}
+    groups = [range(0, 6), range(6, 9), range(9, 12), [12], [13, 14], range(15, 18), [18], [19, 20], range(21, 24)]
+    s0 = None
+    for eng, nsteps in (("dft", 2), ("tf32x3", 4)):
+        run = KHRun(loads(ini_for(args.workload, "keep", eng)), device=dev)
+        run.init()
+        stream = torch.cuda.Stream(device=dev)
+        if s0 is None:
+            s0 = run.state.clone()
+        t = (C.c_float * 8)()
+        _lib.check(lib.ymkh_stage_times(run.ctx, 1, C.c_void_p(stream.cuda_stream), t, 8), "stage times")
+        _lib.check(lib.ymkh_stage_times(run.ctx, nsteps, C.c_void_p(stream.cuda_stream), t, 8), "stage times")
+        step_ms = sum(t[:7]) / nsteps
+        bands_ms = t[4] / nsteps
+        cells = run.d.nx * run.d.nz
+        bands = run.d.bands
+        flops = sum(2 * 2.0 * (2 * (hi - lo + 1)) * run.d.nx * run.d.nz * 21 for lo, hi in bands)
+        r = {"ms_per_step": step_ms, "cell_steps_per_s": cells / (step_ms / 1e3), "bands_ms": bands_ms,
+             "band_share": bands_ms / step_ms, "bands": bands,
+             "band_algorithmic_tflops": flops / (bands_ms / 1e3) / 1e12}
+        if eng == "tf32x3":
+            peak, kind = measured_tf32_peak()
+            ach = r["band_algorithmic_tflops"]
+            r["roofline"] = {"bound": "tensor", "achieved": ach, "executed": 3 * ach, "peak": peak,
+                             "unit": "TFLOP/s", "frac": 3 * ach / peak, "peak_source": kind}
+        # one step from the common initial state, for the error of TF32 against FP64
+        run.set_state(s0)
+        run.step(1, stream)
+        torch.cuda.synchronize(dev)
+        states[eng] = run.state.clone()
+        out[eng] = r
+        run.close()
+        del run
+        torch.cuda.empty_cache()
+    a, b = states["tf32x3"], states["dft"]
+    num = (a - b).reshape(24, -1).norm(dim=1).cpu().numpy()
+    nrm = b.reshape(24, -1).norm(dim=1).cpu().numpy()
+    raw = np.where(nrm > 0, num / np.where(nrm > 0, nrm, 1), num)
+    grp = np.zeros(24)
+    for g in groups:
+        g = list(g)
+        grp[g] = num[g] / max(nrm[g].max(), 1e-300)
+    out["tf32x3"]["error_vs_dft_after_1_step"] = {"max_raw": float(raw.max()), "max_group": float(grp.max()),
+                                                  "median_raw": float(np.median(raw))}
+    out["tf32x3_over_dft"] = out["dft"]["ms_per_step"] / out["tf32x3"]["ms_per_step"]
+    del states, s0, a, b
+    torch.cuda.empty_cache()
+    return out
 
 
 if __name__ == "__main__":

@@ -225,10 +225,11 @@ enum { YMKH_SNAP_CSV = 0, YMKH_SNAP_FP64 = 1 };
 int ymkh_snapshot(ymkh_ctx* ctx, const char* path, int format, void* stream);
 int ymkh_snapshot_wait(ymkh_ctx* ctx);
 
-/* Reports (and clears) a failure of the bounded waits inside the kernels
- * (a staged row that never arrived): YMKH_ECUDA if one timed out since the
- * last check.  Synchronises `stream`; ymkh_energy calls it.  No reference
- * counterpart. */
+/* Reports (and clears) the device error word: YMKH_ECUDA if a bounded wait
+ * inside a kernel timed out (a staged row that never arrived,
+ * YMKH_ERR_WAIT) or, in the debug build, an out-of-range access was skipped
+ * (YMKH_ERR_BOUNDS) since the last check.  Synchronises `stream`;
+ * ymkh_energy calls it.  No reference counterpart. */
 int ymkh_check(ymkh_ctx* ctx, void* stream);
 
 /* Frees the context (not the bound state). */
@@ -261,6 +262,16 @@ int ymkh_batch_destroy(ymkh_batch* batch);
 /* Number of kernel launches issued by this library since load (all entry
  * points, all threads).  Used to report launch counts. */
 long long ymkh_launch_count(void);
+
+/* How the loaded library was built (no reference counterpart): a bit set of
+ * YMKH_BUILD_DEBUG, set in libymkh_debug.so, whose fused kernels check every
+ * global row copy and store against its array before making it; a failed
+ * check skips the access and sets YMKH_ERR_BOUNDS in the error word that
+ * ymkh_check / ymkh_batch_check report.  Nothing traps. */
+#define YMKH_BUILD_DEBUG 1
+#define YMKH_ERR_WAIT 1u   /* error word: a bounded in-kernel wait ran out */
+#define YMKH_ERR_BOUNDS 2u /* error word (debug build): an out-of-range access was skipped */
+int ymkh_build_flags(void);
 
 /* Total energy of a caller-bound state without any device allocation by the
  * library (no context; no reference counterpart: the reference sums energy

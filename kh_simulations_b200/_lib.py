@@ -10,12 +10,15 @@ from pathlib import Path
 
 _PKG = Path(__file__).resolve().parent
 LIB_PATH = _PKG / "libymkh.so"
+DEBUG_LIB_PATH = _PKG / "libymkh_debug.so"  # the same library with checked accesses (YMKH_DEBUG)
 
 NFIELDS, NFLUID, NSTATE = 12, 6, 24
 MAX_EXTRA_BANDS = 4
 NOALLOC_MAX_CELLS = 134217728  # YMKH_NOALLOC_MAX_CELLS
 FILTER_DFT, FILTER_TF32X3 = 0, 1
 FCT_FUSED, FCT_SPLIT = 0, 1
+YMKH_BUILD_DEBUG = 1  # ymkh_build_flags(): the library's kernels check their accesses
+ERR_WAIT, ERR_BOUNDS = 1, 2  # bits of the device error word
 PAIRS = {"Az": 0, "By": 1, "Ex": 2, "Ez": 3}  # YMKH_PAIR_*
 GAUSS_NOUT = 16  # YMKH_GAUSS_NOUT
 SNAP_CSV, SNAP_FP64 = 0, 1
@@ -103,6 +106,7 @@ _SIGS = {
     "ymkh_batch_destroy": (C.c_int, [C.c_void_p]),
     "ymkh_twiddles": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "ymkh_launch_count": (C.c_longlong, []),
+    "ymkh_build_flags": (C.c_int, []),
     "ymkh_energy_noalloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "ymkh_stage_times": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_float), C.c_int]),
 }

@@ -34,10 +34,13 @@ def sources() -> list[Path]:
     return sorted(CSRC.glob("*.cu"))
 
 
-def _stale() -> bool:
-    if not LIB.exists():
+DEBUG_LIB = PKG / "libymkh_debug.so"
+
+
+def _stale(lib: Path = LIB) -> bool:
+    if not lib.exists():
         return True
-    t = LIB.stat().st_mtime
+    t = lib.stat().st_mtime
     deps = sources() + sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
     return any(p.stat().st_mtime > t for p in deps)
 
@@ -47,11 +50,15 @@ def nvcc() -> str:
     return cand if Path(cand).exists() else "nvcc"
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compile csrc/*.cu into libymkh.so (skipped when up to date)."""
-    if not force and not _stale():
-        return LIB
-    cmd = [nvcc(), *NVCC_FLAGS, f"-I{INCLUDE}", *map(str, sources()), "-o", str(LIB)]
+def build(force: bool = False, verbose: bool = False, debug: bool = False) -> Path:
+    """Compile csrc/*.cu into libymkh.so (skipped when up to date); with
+    debug, into libymkh_debug.so with the kernels' access checks on
+    (-DYMKH_DEBUG=1)."""
+    lib = DEBUG_LIB if debug else LIB
+    if not force and not _stale(lib):
+        return lib
+    cmd = [nvcc(), *NVCC_FLAGS, *(["-DYMKH_DEBUG=1"] if debug else []), f"-I{INCLUDE}", *map(str, sources()),
+           "-o", str(lib)]
     if verbose:
         print(" ".join(cmd), flush=True)
     res = subprocess.run(cmd, capture_output=True, text=True)
@@ -59,9 +66,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         raise RuntimeError(f"nvcc failed ({res.returncode}):\n{res.stderr}\n{res.stdout}")
     if verbose and res.stderr.strip():
         print(res.stderr, file=sys.stderr)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True)
-    print(LIB)
+    print(build(force="--force" in sys.argv, verbose=True, debug="--debug" in sys.argv))

@@ -467,6 +467,8 @@ int ymkh_last_error(char* buf, size_t n) {
 
 long long ymkh_launch_count(void) { return g_launches.load(); }
 
+int ymkh_build_flags(void) { return YMKH_DEBUG ? YMKH_BUILD_DEBUG : 0; }
+
 int ymkh_create(const ymkh_grid* grid, const ymkh_params* params, ymkh_ctx** out) {
   if (!grid || !params || !out) return set_err(YMKH_EINVAL, "null argument");
   if (grid->nx < 4 || grid->nz < 4) return set_err(YMKH_EINVAL, "grid too small (%d x %d)", grid->nx, grid->nz);
@@ -583,7 +585,9 @@ int ymkh_check(ymkh_ctx* c, void* stream) {
   CK(cudaStreamSynchronize((cudaStream_t)stream), "error word sync");
   if (h) {
     cudaMemsetAsync(c->derr, 0, sizeof(unsigned), (cudaStream_t)stream);
-    return set_err(YMKH_ECUDA, "a bounded in-kernel wait timed out (error word %u); results of that step are invalid", h);
+    return set_err(YMKH_ECUDA, "%s (error word %u); results of that step are invalid",
+                   (h & ERR_BOUNDS) ? "a checked access was out of range and skipped" : "a bounded in-kernel wait timed out",
+                   h);
   }
   return 0;
 }
@@ -1071,7 +1075,9 @@ int ymkh_batch_check(ymkh_batch* b, void* stream) {
   CK(cudaStreamSynchronize((cudaStream_t)stream), "error word sync");
   if (h) {
     cudaMemsetAsync(b->derr, 0, sizeof(unsigned), (cudaStream_t)stream);
-    return set_err(YMKH_ECUDA, "a bounded in-kernel wait timed out (error word %u)", h);
+    return set_err(YMKH_ECUDA, "%s (error word %u)",
+                   (h & ERR_BOUNDS) ? "a checked access was out of range and skipped" : "a bounded in-kernel wait timed out",
+                   h);
   }
   return 0;
 }

@@ -11,8 +11,8 @@
 //   G[z, x] = G[z, x] - sum_j W[z, j] C[j, x]       (subtract the band)
 // with W[z, 2i] = cosf(phase), W[z, 2i+1] = sinf(phase) the reference's FP32
 // twiddles (YM_Physics.cu:387-388) widened to double and inv2 = 2.0f/nz
-// (:425).  Summation order differs from the reference's warp-shuffle tree;
-// the result agrees to rounding.
+// (:425), summed in the reference's order (its warp-shuffle tree), so the
+// filtered step is bit-identical to the reference's -fmad=false build.
 
 #include "ymkh_common.cuh"
 
@@ -169,91 +169,165 @@ cudaError_t prepare_column(int nz) {
   return cudaSuccess;
 }
 
-// ------------------------------------------------------------- band GEMMs
-// Register-blocked FP64 contractions, 64x64 output tiles, 256 threads with a
-// 4x4 micro-tile each, K staged through shared memory 16 at a time.
-constexpr int GB = 64, GK = 16;
+// ------------------------------------------------------------- band filter
+// The FP64 band filter in the reference's own summation order, so that a
+// filtered step is bit-identical to the reference's kernels built with
+// -fmad=false (YM_Physics.cu:349-455 for the 15 EM/colour arrays, :461-584
+// for pz, px and n).  Two dense contractions per band and array, each
+// blocked over (mode, column) or (z, column) tiles:
+//
+//   coefficients  C[j][x] = inv2 * S_j(x),
+//     S_j(x) = sum over warps w, in order from 0.0, of the warp's lane-0
+//     shuffle tree of the 32 products v[32w + i][x] * tw[j][32w + i]
+//     (YM_Physics.cu:396-426);
+//   apply         v[z][x] -= delta, delta = sum over modes m in order from
+//     0.0 of (A_m * cos_m(z) + B_m * sin_m(z)) (YM_Physics.cu:429-450).
+//
+// Products and sums are rounded separately (no fused multiply-add), as the
+// reference's -fmad=false build rounds them.
 
-// C_k[j, x] = inv2 * sum_z W[z, j] * G_k[z, x];  j in [0, J), W row stride ldw.
-__global__ void __launch_bounds__(256)
+// The reference's warp reduction (shfl_down by 16, 8, 4, 2, 1) leaves lane 0
+// with root = T4(0) + T4(1), T4(i) = T3(i) + T3(i+2), T3(i) = T2(i) + T2(i+4),
+// T2(i) = T1(i) + T1(i+8), T1(i) = a_i + a_{i+16} (every sum is commutative,
+// so only the grouping matters).  Visited in bit-reversed order (0, 8, 4,
+// 12, 2, ...), the sixteen T1 nodes form a balanced pairwise tree over
+// consecutive visits, which a stack of four partial sums evaluates.
+__host__ __device__ constexpr int bitrev4(int k) {
+  return ((k & 1) << 3) | ((k & 2) << 1) | ((k & 4) >> 1) | ((k & 8) >> 3);
+}
+
+constexpr int BC_TJ = 32, BC_TX = 64, BC_CH = 32;  // coefficient tile: 32 j (16 modes) x 64 columns, z chunks of 32
+constexpr int BC_RJ = 2, BC_RX = 4;                // per thread: one mode's (cos, sin) x 4 columns
+constexpr int BC_THREADS = (BC_TJ / BC_RJ) * (BC_TX / BC_RX);  // 256
+
+__global__ void __launch_bounds__(BC_THREADS, 2)
     band_coef_kernel(const __grid_constant__ ArrayList arrs, const double* __restrict__ W, int ldw, int J,
                      double* __restrict__ C, int nx, int nz, double inv2) {
-  __shared__ double sW[GK][GB + 1];
-  __shared__ double sG[GK][GB + 1];
-  const int j0 = blockIdx.x * GB, x0 = blockIdx.y * GB, k = blockIdx.z;
+  __shared__ __align__(16) double sW[2][BC_CH][BC_TJ];  // [z][j]
+  __shared__ __align__(16) double sF[2][BC_CH][BC_TX];  // [z][x]
+  const int j0 = blockIdx.x * BC_TJ, x0 = blockIdx.y * BC_TX, k = blockIdx.z;
   const double* G = arrs.p[k];
   double* Ck = C + (size_t)k * J * nx;
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;  // ty -> j, tx -> x
-  double acc[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-  for (int z0 = 0; z0 < nz; z0 += GK) {
-    for (int i = threadIdx.x; i < GK * GB; i += 256) {
-      const int zz = i / GB, c = i - zz * GB;
-      const int z = z0 + zz;
-      sW[zz][c] = (z < nz && j0 + c < J) ? W[(size_t)z * ldw + j0 + c] : 0.0;
-      sG[zz][c] = (z < nz && x0 + c < nx) ? G[idx2(x0 + c, z, nx)] : 0.0;
+  const int tj = threadIdx.x % (BC_TJ / BC_RJ);  // mode of the tile
+  const int tx = threadIdx.x / (BC_TJ / BC_RJ);  // group of 4 columns
+  const int nch = (nz + BC_CH - 1) / BC_CH;
+
+  auto stage = [&](int buf, int ch) {
+    // 32 z rows of W (32 j) and of the array (64 x): 16-byte pieces where
+    // aligned and in range, else element by element with zero padding
+    for (int i = threadIdx.x; i < BC_CH * BC_TJ; i += BC_THREADS) {
+      const int zz = i / BC_TJ, c = i - zz * BC_TJ, z = ch * BC_CH + zz;
+      sW[buf][zz][c] = (z < nz && j0 + c < J) ? W[(size_t)z * ldw + j0 + c] : 0.0;
     }
-    __syncthreads();
+    for (int i = threadIdx.x; i < BC_CH * BC_TX; i += BC_THREADS) {
+      const int zz = i / BC_TX, c = i - zz * BC_TX, z = ch * BC_CH + zz;
+      sF[buf][zz][c] = (z < nz && x0 + c < nx) ? G[idx2(x0 + c, z, nx)] : 0.0;
+    }
+  };
+
+  double S[BC_RJ][BC_RX];
 #pragma unroll
-    for (int zz = 0; zz < GK; ++zz) {
-      double w[4], gv[4];
+  for (int a = 0; a < BC_RJ; ++a)
 #pragma unroll
-      for (int a = 0; a < 4; ++a) w[a] = sW[zz][ty + 16 * a];
+    for (int b = 0; b < BC_RX; ++b) S[a][b] = 0.0;
+
+  stage(0, 0);
+  __syncthreads();
+  for (int ch = 0; ch < nch; ++ch) {
+    const int buf = ch & 1;
+    if (ch + 1 < nch) stage(buf ^ 1, ch + 1);  // the other buffer was released by the barrier below
+    double st[4][BC_RJ][BC_RX];  // pending tree nodes of heights 1..4 (T2..T4 partial sums)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) gv[b] = sG[zz][tx + 16 * b];
+    for (int kk = 0; kk < 16; ++kk) {
+      const int i = bitrev4(kk);
+      double w0[BC_RJ], w1[BC_RJ], f0[BC_RX], f1[BC_RX];
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < BC_RJ; ++a) {
+        w0[a] = sW[buf][i][tj * BC_RJ + a];
+        w1[a] = sW[buf][i + 16][tj * BC_RJ + a];
+      }
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(w[a], gv[b], acc[a][b]);
+      for (int b = 0; b < BC_RX; ++b) {
+        f0[b] = sF[buf][i][tx * BC_RX + b];
+        f1[b] = sF[buf][i + 16][tx * BC_RX + b];
+      }
+#pragma unroll
+      for (int a = 0; a < BC_RJ; ++a)
+#pragma unroll
+        for (int b = 0; b < BC_RX; ++b) {
+          const double p0 = f0[b] * w0[a];  // YM_Physics.cu:394 ar = v * cz (rounded)
+          const double p1 = f1[b] * w1[a];
+          double x = p0 + p1;  // T1(i)
+          // merge with the pending nodes: one level per trailing one bit of kk
+          int lvl = 0;
+#pragma unroll
+          for (int L = 0; L < 4; ++L) {
+            if (((kk >> L) & 1) && lvl == L) {
+              x = st[L][a][b] + x;
+              ++lvl;
+            }
+          }
+          if (lvl < 4) st[lvl][a][b] = x;
+          else S[a][b] = S[a][b] + x;  // warp sums added in warp order from 0.0
+        }
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < BC_RJ; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int j = j0 + ty + 16 * a, x = x0 + tx + 16 * b;
-      if (j < J && x < nx) Ck[(size_t)j * nx + x] = acc[a][b] * inv2;
+    for (int b = 0; b < BC_RX; ++b) {
+      const int j = j0 + tj * BC_RJ + a, x = x0 + tx * BC_RX + b;
+      if (j < J && x < nx) Ck[(size_t)j * nx + x] = S[a][b] * inv2;
     }
 }
 
-// G_k[z, x] -= sum_j W[z, j] * C_k[j, x]
-__global__ void __launch_bounds__(256)
+constexpr int BA_TZ = 64, BA_TX = 64, BA_KM = 16;  // apply tile: 64 z x 64 columns, 16 modes staged at a time
+constexpr int BA_THREADS = 256;                     // 4 x 4 outputs per thread
+
+// v[z][x] -= sum over the band's modes in order of (A_m cos_m(z) + B_m sin_m(z))
+__global__ void __launch_bounds__(BA_THREADS, 2)
     band_apply_kernel(const __grid_constant__ ArrayList arrs, const double* __restrict__ W, int ldw, int J,
                       const double* __restrict__ C, int nx, int nz) {
-  __shared__ double sW[GK][GB + 1];  // [j][z]
-  __shared__ double sC[GK][GB + 1];  // [j][x]
-  const int z0 = blockIdx.x * GB, x0 = blockIdx.y * GB, k = blockIdx.z;
+  __shared__ __align__(16) double sW[2 * BA_KM][BA_TZ + 1];  // [j][z]
+  __shared__ __align__(16) double sC[2 * BA_KM][BA_TX + 1];  // [j][x]
+  const int z0 = blockIdx.x * BA_TZ, x0 = blockIdx.y * BA_TX, k = blockIdx.z;
   double* G = arrs.p[k];
   const double* Ck = C + (size_t)k * J * nx;
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;  // ty -> z, tx -> x
-  double acc[4][4];
+  double delta[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-  for (int jb = 0; jb < J; jb += GK) {
-    for (int i = threadIdx.x; i < GK * GB; i += 256) {
-      const int jj = i / GB, c = i - jj * GB;
+    for (int b = 0; b < 4; ++b) delta[a][b] = 0.0;
+  for (int jb = 0; jb < J; jb += 2 * BA_KM) {
+    for (int i = threadIdx.x; i < 2 * BA_KM * BA_TZ; i += BA_THREADS) {
+      const int jj = i / BA_TZ, c = i - jj * BA_TZ;
       const int j = jb + jj;
       sW[jj][c] = (j < J && z0 + c < nz) ? W[(size_t)(z0 + c) * ldw + j] : 0.0;
       sC[jj][c] = (j < J && x0 + c < nx) ? Ck[(size_t)j * nx + x0 + c] : 0.0;
     }
     __syncthreads();
+    const int mend = min(BA_KM, (J - jb) / 2);
+    for (int mm = 0; mm < mend; ++mm) {
+      double wc[4], ws[4], ca[4], cb[4];
 #pragma unroll
-    for (int jj = 0; jj < GK; ++jj) {
-      double w[4], cv[4];
+      for (int a = 0; a < 4; ++a) {
+        wc[a] = sW[2 * mm][ty + 16 * a];
+        ws[a] = sW[2 * mm + 1][ty + 16 * a];
+      }
 #pragma unroll
-      for (int a = 0; a < 4; ++a) w[a] = sW[jj][ty + 16 * a];
-#pragma unroll
-      for (int b = 0; b < 4; ++b) cv[b] = sC[jj][tx + 16 * b];
+      for (int b = 0; b < 4; ++b) {
+        ca[b] = sC[2 * mm][tx + 16 * b];
+        cb[b] = sC[2 * mm + 1][tx + 16 * b];
+      }
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(w[a], cv[b], acc[a][b]);
+        for (int b = 0; b < 4; ++b) {
+          const double t = ca[b] * wc[a] + cb[b] * ws[a];  // YM_Physics.cu:433 A_m cz + B_m sz
+          delta[a][b] = delta[a][b] + t;
+        }
     }
     __syncthreads();
   }
@@ -264,19 +338,19 @@ __global__ void __launch_bounds__(256)
       const int z = z0 + ty + 16 * a, x = x0 + tx + 16 * b;
       if (z < nz && x < nx) {
         const size_t gi = idx2(x, z, nx);
-        G[gi] = G[gi] - acc[a][b];
+        G[gi] = G[gi] - delta[a][b];
       }
     }
 }
 
 cudaError_t launch_band(const ArrayList& arrs, int narr, const double* W, int ldw, int J, double* C, int nx, int nz,
                         double inv2, cudaStream_t s) {
-  dim3 g1((J + GB - 1) / GB, (nx + GB - 1) / GB, narr);
-  band_coef_kernel<<<g1, 256, 0, s>>>(arrs, W, ldw, J, C, nx, nz, inv2);
+  dim3 g1((J + BC_TJ - 1) / BC_TJ, (nx + BC_TX - 1) / BC_TX, narr);
+  band_coef_kernel<<<g1, BC_THREADS, 0, s>>>(arrs, W, ldw, J, C, nx, nz, inv2);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  dim3 g2((nz + GB - 1) / GB, (nx + GB - 1) / GB, narr);
-  band_apply_kernel<<<g2, 256, 0, s>>>(arrs, W, ldw, J, C, nx, nz);
+  dim3 g2((nz + BA_TZ - 1) / BA_TZ, (nx + BA_TX - 1) / BA_TX, narr);
+  band_apply_kernel<<<g2, BA_THREADS, 0, s>>>(arrs, W, ldw, J, C, nx, nz);
   return cudaGetLastError();
 }
 

@@ -11,7 +11,34 @@
 #include <string>
 #include "../../include/ymkh.h"
 
+// Debug build (nvcc -DYMKH_DEBUG=1, built as libymkh_debug.so): the fused
+// kernels check every global row copy and every global store against the
+// extent of its array, and every staged row against its shared-memory
+// slot, before making it.  A failed check sets ERR_BOUNDS in the device
+// error word (reported by ymkh_check) and the access is skipped: nothing
+// traps or asserts.  Release builds compile the checks away.
+#ifndef YMKH_DEBUG
+#define YMKH_DEBUG 0
+#endif
+
 namespace ymkh {
+
+constexpr unsigned ERR_WAIT = 1u;    // a bounded in-kernel wait ran out of polls
+constexpr unsigned ERR_BOUNDS = 2u;  // debug build: an access outside its array was skipped
+
+// true if the access may be made; in a debug build a false `ok` is recorded
+__device__ __forceinline__ bool dbg_ok(bool ok, unsigned* err) {
+#if YMKH_DEBUG
+  if (!ok) {
+    if (err) atomicOr(err, ERR_BOUNDS);
+    return false;
+  }
+#else
+  (void)ok;
+  (void)err;
+#endif
+  return true;
+}
 
 // State order of include/ymkh.h.
 enum Field { EX1 = 0, EX2, EX3, EZ1, EZ2, EZ3, BY1, BY2, BY3, AZ1, AZ2, AZ3 };
@@ -226,7 +253,7 @@ __device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned phase, unsigne
         : "memory");
     if (done) return;
   }
-  if (err) atomicOr(err, 1u);
+  if (err) atomicOr(err, ERR_WAIT);
 }
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
   unsigned d = (unsigned)__cvta_generic_to_shared(dst);

@@ -218,16 +218,20 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
         // and the phase cannot complete before that arrival.  The copy's
         // array, slot and wrap split are fixed per item (cp_*).
         if (tid == 0) mbar_expect_tx(&bars[s], (unsigned)(narr * W * 8));
-        if (cp_base) {
+        if (cp_base && dbg_ok(zr >= 0 && zr < nz && zm >= 0 && zm < nz && zp >= 0 && zp < nz && cp_x1 >= 0 &&
+                                  cp_len1 > 0 && cp_x1 + cp_len1 <= nx && W - cp_len1 <= nx && cp_dst >= 0 &&
+                                  cp_dst < ST_SIZE, T.err)) {
           const size_t off = cp_kind == 0 ? ro : (cp_kind == 1 ? rom : rop);
           double* const dst = sb + cp_dst * W;
           bulk_g2s(dst, cp_base + off + cp_x1, (unsigned)cp_len1 * 8u, &bars[s]);
           if (cp_len1 < W) bulk_g2s(dst + cp_len1, cp_base + off, (unsigned)(W - cp_len1) * 8u, &bars[s]);
         }
       } else {
+        const bool rows_ok = dbg_ok(zr >= 0 && zr < nz && zm >= 0 && zm < nz && zp >= 0 && zp < nz, T.err);
         for (int i = tid; i < 12 * (W - 1); i += NT) {
           const int a = i / (W - 1), q = 1 + (i - a * (W - 1));
-          cp_async8(sb + (ST_FL + a) * W + q, (a < 6 ? st.a[a] : st.b[a - 6]) + ro + xtab[q]);
+          if (rows_ok && dbg_ok(xtab[q] >= 0 && xtab[q] < nx, T.err))
+            cp_async8(sb + (ST_FL + a) * W + q, (a < 6 ? st.a[a] : st.b[a - 6]) + ro + xtab[q]);
         }
         for (int i = tid; i < 21 * (W - 1); i += NT) {
           const int a = i / (W - 1), q = 1 + (i - a * (W - 1));
@@ -237,13 +241,15 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
                                : (kind <= 4) ? st.f[EZ1 + c]
                                              : st.f[AZ1 + c];
           const size_t off = (kind == 2 || kind == 4 || kind == 6) ? rom : ro;
-          cp_async8(sb + (ST_EX + a) * W + q, base + off + xtab[q]);
+          if (rows_ok && dbg_ok(xtab[q] >= 0 && xtab[q] < nx, T.err))
+            cp_async8(sb + (ST_EX + a) * W + q, base + off + xtab[q]);
         }
         if (warm) {
           for (int i = tid; i < 4 * (W - 1); i += NT) {
             const int a = i / (W - 1), q = 1 + (i - a * (W - 1));
             const double* base = (a & 1) ? st.b[FN] : st.a[FN];
-            cp_async8(sb + (ST_NZP + a) * W + q, base + ((a >> 1) ? rom : rop) + xtab[q]);
+            if (rows_ok && dbg_ok(xtab[q] >= 0 && xtab[q] < nx, T.err))
+              cp_async8(sb + (ST_NZP + a) * W + q, base + ((a >> 1) ? rom : rop) + xtab[q]);
           }
         }
         cp_async_commit();
@@ -436,8 +442,10 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
           }
           double* const* dst = beam ? out.b : out.a;
           const size_t gi = idx2(x_own, o, nx);
+          if (dbg_ok(x_own >= 0 && x_own < nx && o >= 0 && o < nz && sp >= 1 && sp + 2 < W, T.err)) {
 #pragma unroll
-          for (int j = 0; j < 3; ++j) dst[k0 + j][gi] = outv[j];
+            for (int j = 0; j < 3; ++j) dst[k0 + j][gi] = outv[j];
+          }
         }
       }
     }

@@ -134,11 +134,13 @@ __global__ void __launch_bounds__(MX_NT, YMKH_MX_MINB)
         // thread 0's arrival arms the phase
         if (tid == 0) mbar_expect_tx(&bars[s], (unsigned)(MS_SIZE * W * 8));
         const int a = (tid & 31) * (NT / 32) + (tid >> 5);
-        if (a < MS_SIZE) bulk_row_periodic(sb + a * W, arr(a) + ro, x0 - 2, W, nx, &bars[s]);
+        if (a < MS_SIZE && dbg_ok(zwrap(q, nz) >= 0 && zwrap(q, nz) < nz && W <= nx && (x0 - 2) % 2 == 0, T.err))
+          bulk_row_periodic(sb + a * W, arr(a) + ro, x0 - 2, W, nx, &bars[s]);
       } else {
         for (int i = tid; i < MS_SIZE * W; i += NT) {
           const int a = i / W, k = i - a * W;
-          cp_async8(sb + a * W + k, arr(a) + ro + xtab[k]);
+          if (dbg_ok(zwrap(q, nz) >= 0 && zwrap(q, nz) < nz && xtab[k] >= 0 && xtab[k] < nx, T.err))
+            cp_async8(sb + a * W + k, arr(a) + ro + xtab[k]);
         }
         cp_async_commit();
       }
@@ -246,7 +248,8 @@ __global__ void __launch_bounds__(MX_NT, YMKH_MX_MINB)
       // Ex and Ez of column x0+tid-64.
       const int o = q - 1;
       const int c3 = tid < NT / 2 ? tid : tid - NT / 2;
-      if (c3 < TX && o >= zs && o < ze && x0 + c3 < nx) {
+      if (c3 < TX && o >= zs && o < ze && x0 + c3 < nx &&
+          dbg_ok(x0 + c3 >= 0 && o >= 0 && o < nz && 2 + c3 + 1 < W, T.err)) {
         const int k = 2 + c3;
         const size_t gi = idx2(x0 + c3, o, nx);
         double ex[3], ez[3];

@@ -149,8 +149,12 @@ class KHRun:
             profiles = load_profiles(seed_file, d.nx) if seed_file else None
         ip, keep = init_params(cfg, d, profiles)
         with torch.cuda.device(self.device):
+            cur = torch.cuda.current_stream(self.device)
+            if stream is not None:  # after the buffers' zero fill on torch's current stream
+                stream.wait_stream(cur)
             check(self.lib.ymkh_init(self.ctx, C.byref(ip), C.c_void_p(_stream_ptr(stream))), "ymkh_init")
-            torch.cuda.synchronize(self.device)
+            # the state is ready on return; other streams' work is not waited for
+            (stream if stream is not None else cur).synchronize()
         self.step_count = 0
         self.history.clear()
         self.halted = False

@@ -61,7 +61,7 @@ class KHRequest:
     arrival: float = 0.0           # seconds after the server starts
     admitted: float = math.nan
     finished: float = math.nan
-    status: str = "pending"        # pending | running | done | halted | rejected | cancelled
+    status: str = "pending"        # pending | running | done | halted | rejected | cancelled | unfinished
     cancel_at: float = math.inf    # seconds after the server starts: withdrawn from then on
     energy: float = math.nan
     state: np.ndarray | None = None
@@ -93,6 +93,7 @@ class ServeReport:
     def summary(self) -> dict:
         n_done = sum(r.status in ("done", "halted") for r in self.requests)
         return {"mode": self.mode, "requests": len(self.requests), "completed": n_done,
+                "unfinished": sum(r.status == "unfinished" for r in self.requests),
                 "halted": sum(r.status == "halted" for r in self.requests),
                 "rejected": sum(r.status == "rejected" for r in self.requests),
                 "cancelled": sum(r.status == "cancelled" for r in self.requests),
@@ -101,8 +102,18 @@ class ServeReport:
                 **self.extra}
 
 
+def _censor(reqs, end: float) -> None:
+    """Requests that had arrived by `end` but never ran to the end are
+    "unfinished", their latency censored at `end`."""
+    for r in reqs:
+        if r.status in ("pending", "running") and r.arrival <= end:
+            r.status, r.finished = "unfinished", end
+
+
 def _percentiles(reqs) -> tuple:
-    lat = [r.latency for r in reqs if r.status in ("done", "halted")]
+    """p50 / p99 latency over completed requests and over unfinished ones at
+    their censored latency (so, with any unfinished, lower bounds)."""
+    lat = [r.latency for r in reqs if r.status in ("done", "halted", "unfinished")]
     if not lat:
         return math.nan, math.nan
     return float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
@@ -114,10 +125,17 @@ class KHServer:
     budget_bytes: device memory the resident runs may hold together.
     chunk: steps between admission/retirement decisions.
     keep_state: copy each finished run's final state to the host.
+    large_cells: runs of at least this many cells fill the GPU on their own
+        (one persistent FCT/Maxwell kernel over their tiles already occupies
+        every SM, and the lone-run schedule of 128-wide strips in contiguous
+        blocks is faster than a batch's): they are stepped one at a time in
+        arrival order, in turns with the smaller runs, which advance
+        together as one batch.  0 batches every run.
     """
 
     def __init__(self, budget_bytes: int, device="cuda", chunk: int = 100, graph_steps: int = 4,
-                 keep_state: bool = False, check_energy: bool = True, clock=time.perf_counter):
+                 keep_state: bool = False, check_energy: bool = True, clock=time.perf_counter,
+                 large_cells: int = 1 << 20):
         self.budget = int(budget_bytes)
         self.device = device
         self.chunk = int(chunk)
@@ -125,14 +143,15 @@ class KHServer:
         self.keep_state = keep_state
         self.check_energy = check_energy
         self.clock = clock
+        self.large_cells = int(large_cells)
 
     # ---------------------------------------------------------------- helpers
-    def _start_run(self, req: KHRequest):
+    def _start_run(self, req: KHRequest, stream=None):
         from .run import KHRun
 
         run = KHRun(req.cfg, device=self.device, graph_steps=self.graph_steps)
-        run.init()
-        run.E0 = run.energy()
+        run.init(stream=stream)
+        run.E0 = run.energy(stream)
         return run
 
     def _finish(self, req: KHRequest, run, status: str, t: float):
@@ -161,70 +180,128 @@ class KHServer:
             out.append((req, fp))
         return out
 
+    def _halted(self, run, stream) -> bool:
+        if not self.check_energy:
+            return False
+        e = run.energy(stream)
+        return not math.isfinite(e) or e / run.E0 > run.d.energy_thresh
+
     # ------------------------------------------------------------------ serve
-    def serve(self, requests: list) -> ServeReport:
+    def serve(self, requests: list, deadline: float = math.inf) -> ServeReport:
+        """Serve `requests` (arrival times in seconds after the start).
+
+        Small runs (below large_cells) join one KHBatch as they are admitted
+        and leave it when done; large runs wait resident in HBM and the
+        oldest is stepped alone.  Each round enqueues up to `chunk` steps of
+        the batch and then up to `chunk` steps of the oldest large run;
+        while they run, arrived requests are admitted and initialised
+        on a separate stream; finished and halted runs retire between
+        rounds.  With a finite `deadline` (seconds after the start) the
+        server stops there: unfinished runs count the steps they made and
+        are reported as "unfinished" (their latency is censored at the
+        deadline)."""
         import torch
 
         from .batch import KHBatch
 
-        stream = torch.cuda.Stream(device=self.device)
+        # the batch and the oldest large run share one stream and take turns:
+        # a large run's persistent kernels give each CTA one contiguous block
+        # of work, so kernels of another stream holding some SMs would delay
+        # the whole launch
+        s_run = torch.cuda.Stream(device=self.device)
+        s_small = s_large = s_run
+        s_admit = torch.cuda.Stream(device=self.device)
         batch = KHBatch(device=self.device, graph_steps=self.graph_steps)
         pending = deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
-        active: list = []  # (req, run, fp, remaining)
+        small: list = []   # [req, run, fp, remaining]
+        large: deque = deque()
         used = 0
         cell_steps = 0
         t0 = self.clock()
         first = pending[0].arrival if pending else 0.0
-        while pending or active:
+        while pending or small or large:
             now = self.clock() - t0
+            if now >= deadline:
+                break
             for req in [r for r in pending if r.cancel_at <= now]:  # withdrawn before admission
                 pending.remove(req)
                 req.status, req.finished = "cancelled", now
+            # this round's work on the resident runs
+            ks = min(self.chunk, min(a[3] for a in small)) if small else 0
+            kl, head = 0, None
+            if large:
+                head = large[0]
+                kl = min(self.chunk, head[3])
+            if ks:
+                batch.step(ks, s_small)
+            if kl:
+                head[1].step(kl, s_large)
+            # admissions while the device works; new runs start on their own stream
+            admitted = []
             for req, fp in self.admit_order(pending, now, used):
-                run = self._start_run(req)
+                run = self._start_run(req, s_admit)
                 req.admitted = self.clock() - t0
                 req.status = "running"
-                batch.add(run)
-                active.append([req, run, fp, req.steps])
+                admitted.append([req, run, fp, req.steps])
                 used += fp
-            if not active:
+            if not ks and not kl and not admitted:
                 if pending:
                     time.sleep(max(0.0, min(0.05, pending[0].arrival - (self.clock() - t0))))
                 continue
-            k = min(self.chunk, min(a[3] for a in active))
-            batch.step(k, stream)
-            stream.synchronize()
-            for a in active:
-                a[3] -= k
-                cell_steps += k * a[0].cells
-            keep = []
-            for a in active:
+            s_run.synchronize()
+            for a in small:
+                a[3] -= ks
+                cell_steps += ks * a[0].cells
+            if kl:
+                head[3] -= kl
+                cell_steps += kl * head[0].cells
+            t = self.clock() - t0
+            done, keep = [], []
+            for a in small:
                 req, run, fp, rem = a
-                status = None
-                if rem <= 0:
-                    status = "done"
-                elif req.cancel_at <= self.clock() - t0:
-                    status = "cancelled"  # withdrawn mid-flight: slot and memory freed
-                elif self.check_energy:
-                    e = run.energy(stream)
-                    if not math.isfinite(e) or e / run.E0 > run.d.energy_thresh:
-                        status = "halted"
+                status = ("done" if rem <= 0 else "cancelled" if req.cancel_at <= t
+                          else "halted" if ks and self._halted(run, s_small) else None)
                 if status:
                     batch.remove(run)
-                    self._finish(req, run, status, self.clock() - t0)
-                    used -= fp
+                    done.append((a, status))
                 else:
                     keep.append(a)
-            active = keep
-        makespan = (self.clock() - t0) - first
+            small = keep
+            if kl:
+                req, run, fp, rem = head
+                status = ("done" if rem <= 0 else "cancelled" if req.cancel_at <= t
+                          else "halted" if self._halted(run, s_large) else None)
+                if status:
+                    large.popleft()
+                    done.append((head, status))
+            for a in [a for a in large if a[0].cancel_at <= t]:  # withdrawn while waiting
+                large.remove(a)
+                done.append((a, "cancelled"))
+            for (req, run, fp, _), status in done:
+                self._finish(req, run, status, self.clock() - t0)
+                used -= fp
+            for a in admitted:
+                if self.large_cells > 0 and a[0].cells >= self.large_cells:
+                    large.append(a)
+                else:
+                    batch.add(a[1])
+                    small.append(a)
+        end = self.clock() - t0
+        for req, run, fp, rem in small + list(large):
+            req.status, req.finished = "unfinished", end
+            run.close()
+        _censor(requests, end)
         batch.close()
+        makespan = end - first
         p50, p99 = _percentiles(requests)
-        return ServeReport(requests, makespan, cell_steps, p50, p99, "batched")
+        return ServeReport(requests, makespan, cell_steps, p50, p99, "batched",
+                           {"large_cells": self.large_cells, "unfinished": sum(r.status == "unfinished"
+                                                                              for r in requests)})
 
-    def serve_sequential(self, requests: list) -> ServeReport:
+    def serve_sequential(self, requests: list, deadline: float = math.inf) -> ServeReport:
         """The same requests one by one through the plain single-run step, in
         arrival order (a request starts when it has arrived and the previous
-        one has finished)."""
+        one has finished).  `deadline` as in serve()."""
         import torch
 
         stream = torch.cuda.Stream(device=self.device)
@@ -233,6 +310,8 @@ class KHServer:
         first = order[0].arrival if order else 0.0
         cell_steps = 0
         for req in order:
+            if self.clock() - t0 >= deadline:
+                break
             if footprint(req.cfg) > self.budget:
                 req.status = "rejected"
                 continue
@@ -241,8 +320,10 @@ class KHServer:
                 continue
             now = self.clock() - t0
             if req.arrival > now:
+                if req.arrival >= deadline:
+                    break
                 time.sleep(req.arrival - now)
-            run = self._start_run(req)
+            run = self._start_run(req, stream)
             req.admitted = self.clock() - t0
             status = "done"
             left = req.steps
@@ -250,20 +331,28 @@ class KHServer:
                 if req.cancel_at <= self.clock() - t0:
                     status = "cancelled"
                     break
+                if self.clock() - t0 >= deadline:
+                    status = "unfinished"
+                    break
                 k = min(self.chunk, left)
                 run.step(k, stream)
                 left -= k
                 cell_steps += k * req.cells
-                if self.check_energy:
-                    e = run.energy(stream)
-                    if not math.isfinite(e) or e / run.E0 > run.d.energy_thresh:
-                        status = "halted"
-                        break
+                if self._halted(run, stream):
+                    status = "halted"
+                    break
             stream.synchronize()
-            self._finish(req, run, status, self.clock() - t0)
-        makespan = (self.clock() - t0) - first
+            if status == "unfinished":
+                req.status, req.finished = status, self.clock() - t0
+                run.close()
+            else:
+                self._finish(req, run, status, self.clock() - t0)
+        end = self.clock() - t0
+        _censor(order, end)
+        makespan = end - first
         p50, p99 = _percentiles(order)
-        return ServeReport(order, makespan, cell_steps, p50, p99, "sequential")
+        return ServeReport(order, makespan, cell_steps, p50, p99, "sequential",
+                           {"unfinished": sum(r.status == "unfinished" for r in order)})
 
 
 def poisson_mix(seed: int, rate: float, duration: float, min_cells: int, max_cells: int, min_steps: int,

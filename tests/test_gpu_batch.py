@@ -150,6 +150,24 @@ def test_server_mix_equals_sequential(cuda):
     assert np.isfinite(rep_b.p50) and np.isfinite(rep_b.p99)
 
 
+def test_server_large_runs_alone_equal_sequential(cuda):
+    """Runs at or above large_cells are stepped alone on their own stream
+    beside the batch of the smaller ones; every result still equals the
+    same request run one by one, bit for bit."""
+    from kh_simulations_b200.server import KHRequest, KHServer
+
+    reqs_a = [KHRequest(i, _cfg(t), 24 + 6 * i, arrival=0.005 * i) for i, (t, _) in enumerate(MIX)]
+    reqs_b = [KHRequest(i, _cfg(t), 24 + 6 * i, arrival=0.005 * i) for i, (t, _) in enumerate(MIX)]
+    srv = KHServer(budget_bytes=2 << 30, chunk=8, keep_state=True, check_energy=True, large_cells=8000)
+    rep = srv.serve(reqs_a)
+    srv.serve_sequential(reqs_b)
+    assert sum(r.cells >= 8000 for r in reqs_a) == 2
+    for a, s in zip(sorted(reqs_a, key=lambda r: r.rid), sorted(reqs_b, key=lambda r: r.rid)):
+        assert a.status == s.status == "done"
+        assert np.array_equal(a.state, s.state), a.rid
+    assert rep.extra["unfinished"] == 0
+
+
 def test_autotune_runs_and_keeps_results(cuda, tmp_path, monkeypatch):
     import kh_simulations_b200.autotune as at
     from kh_simulations_b200.run import KHRun

@@ -7,7 +7,7 @@ from collections import deque
 import numpy as np
 
 from kh_simulations_b200.config import loads
-from kh_simulations_b200.server import KHRequest, KHServer, _percentiles, footprint, poisson_mix
+from kh_simulations_b200.server import KHRequest, KHServer, _censor, _percentiles, footprint, poisson_mix
 
 
 def cfg(nz, nx, extra=""):
@@ -77,3 +77,17 @@ def test_percentiles():
         r.finished, r.status = float(i + 1), "done"
     p50, p99 = _percentiles(reqs)
     assert p50 == 3.0 and abs(p99 - np.percentile([1, 2, 3, 4, 5], 99)) < 1e-12
+
+
+def test_censoring_at_a_deadline():
+    """Requests that arrived by the deadline but did not finish are
+    'unfinished' with their latency censored at the deadline (the
+    percentiles are then lower bounds); later arrivals are left out."""
+    reqs = [KHRequest(i, cfg(32, 64), 1, arrival=float(i)) for i in range(4)]
+    reqs[0].status, reqs[0].finished = "done", 0.5
+    reqs[1].status = "running"
+    _censor(reqs, end=2.5)
+    assert [r.status for r in reqs] == ["done", "unfinished", "unfinished", "pending"]
+    assert reqs[1].latency == 1.5 and reqs[2].latency == 0.5
+    p50, _ = _percentiles(reqs)
+    assert p50 == 0.5
