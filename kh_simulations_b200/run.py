@@ -287,9 +287,11 @@ class KHRun:
         torch.cuda.synchronize(self.device)
 
     def close(self) -> None:
+        """Free the context and drop the state buffers (back to torch's cache)."""
         if getattr(self, "ctx", None):
             self.lib.ymkh_destroy(self.ctx)
             self.ctx = None
+        self.buf = []
 
     def __del__(self):  # pragma: no cover
         try:

@@ -147,9 +147,23 @@ class KHServer:
 
     # ---------------------------------------------------------------- helpers
     def _start_run(self, req: KHRequest, stream=None):
+        import torch
+
+        from ._lib import YMKHError
         from .run import KHRun
 
-        run = KHRun(req.cfg, device=self.device, graph_steps=self.graph_steps)
+        run = None
+        try:
+            run = KHRun(req.cfg, device=self.device, graph_steps=self.graph_steps)
+        except (YMKHError, torch.OutOfMemoryError):
+            pass
+        if run is None:
+            # the budget counts live runs, but torch's caching allocator may
+            # still hold the buffers of retired ones (and of the failed
+            # attempt): release them and retry once
+            torch.cuda.synchronize(self.device)
+            torch.cuda.empty_cache()
+            run = KHRun(req.cfg, device=self.device, graph_steps=self.graph_steps)
         run.init(stream=stream)
         run.E0 = run.energy(stream)
         return run
