@@ -213,16 +213,20 @@ __global__ void __launch_bounds__(BC_THREADS, 2)
   const int nch = (nz + BC_CH - 1) / BC_CH;
 
   auto stage = [&](int buf, int ch) {
-    // 32 z rows of W (32 j) and of the array (64 x): 16-byte pieces where
-    // aligned and in range, else element by element with zero padding
+    // 32 z rows of W (32 j) and of the array (64 x), asynchronously (8-byte
+    // cp.async; zero padding past the edges written directly), one commit
+    // group per chunk
     for (int i = threadIdx.x; i < BC_CH * BC_TJ; i += BC_THREADS) {
       const int zz = i / BC_TJ, c = i - zz * BC_TJ, z = ch * BC_CH + zz;
-      sW[buf][zz][c] = (z < nz && j0 + c < J) ? W[(size_t)z * ldw + j0 + c] : 0.0;
+      if (z < nz && j0 + c < J) cp_async8(&sW[buf][zz][c], W + (size_t)z * ldw + j0 + c);
+      else sW[buf][zz][c] = 0.0;
     }
     for (int i = threadIdx.x; i < BC_CH * BC_TX; i += BC_THREADS) {
       const int zz = i / BC_TX, c = i - zz * BC_TX, z = ch * BC_CH + zz;
-      sF[buf][zz][c] = (z < nz && x0 + c < nx) ? G[idx2(x0 + c, z, nx)] : 0.0;
+      if (z < nz && x0 + c < nx) cp_async8(&sF[buf][zz][c], G + idx2(x0 + c, z, nx));
+      else sF[buf][zz][c] = 0.0;
     }
+    cp_async_commit();
   };
 
   double S[BC_RJ][BC_RX];
@@ -232,10 +236,14 @@ __global__ void __launch_bounds__(BC_THREADS, 2)
     for (int b = 0; b < BC_RX; ++b) S[a][b] = 0.0;
 
   stage(0, 0);
-  __syncthreads();
   for (int ch = 0; ch < nch; ++ch) {
     const int buf = ch & 1;
-    if (ch + 1 < nch) stage(buf ^ 1, ch + 1);  // the other buffer was released by the barrier below
+    // the next chunk goes to the other buffer, released by the barrier at
+    // the end of the previous chunk; then this chunk's copies are awaited
+    if (ch + 1 < nch) stage(buf ^ 1, ch + 1);
+    else cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
     double st[4][BC_RJ][BC_RX];  // pending tree nodes of heights 1..4 (T2..T4 partial sums)
 #pragma unroll
     for (int kk = 0; kk < 16; ++kk) {
@@ -282,15 +290,15 @@ __global__ void __launch_bounds__(BC_THREADS, 2)
     }
 }
 
-constexpr int BA_TZ = 64, BA_TX = 64, BA_KM = 16;  // apply tile: 64 z x 64 columns, 16 modes staged at a time
+constexpr int BA_TZ = 64, BA_TX = 64, BA_KM = 8;  // apply tile: 64 z x 64 columns, 8 modes staged at a time
 constexpr int BA_THREADS = 256;                     // 4 x 4 outputs per thread
 
 // v[z][x] -= sum over the band's modes in order of (A_m cos_m(z) + B_m sin_m(z))
 __global__ void __launch_bounds__(BA_THREADS, 2)
     band_apply_kernel(const __grid_constant__ ArrayList arrs, const double* __restrict__ W, int ldw, int J,
                       const double* __restrict__ C, int nx, int nz) {
-  __shared__ __align__(16) double sW[2 * BA_KM][BA_TZ + 1];  // [j][z]
-  __shared__ __align__(16) double sC[2 * BA_KM][BA_TX + 1];  // [j][x]
+  __shared__ __align__(16) double sW[2][2 * BA_KM][BA_TZ + 1];  // [buffer][j][z]
+  __shared__ __align__(16) double sC[2][2 * BA_KM][BA_TX + 1];  // [buffer][j][x]
   const int z0 = blockIdx.x * BA_TZ, x0 = blockIdx.y * BA_TX, k = blockIdx.z;
   double* G = arrs.p[k];
   const double* Ck = C + (size_t)k * J * nx;
@@ -300,26 +308,37 @@ __global__ void __launch_bounds__(BA_THREADS, 2)
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) delta[a][b] = 0.0;
-  for (int jb = 0; jb < J; jb += 2 * BA_KM) {
+  auto stage = [&](int buf, int jb) {  // 8 modes (16 j) of W and of the coefficients, asynchronously
     for (int i = threadIdx.x; i < 2 * BA_KM * BA_TZ; i += BA_THREADS) {
       const int jj = i / BA_TZ, c = i - jj * BA_TZ;
       const int j = jb + jj;
-      sW[jj][c] = (j < J && z0 + c < nz) ? W[(size_t)(z0 + c) * ldw + j] : 0.0;
-      sC[jj][c] = (j < J && x0 + c < nx) ? Ck[(size_t)j * nx + x0 + c] : 0.0;
+      if (j < J && z0 + c < nz) cp_async8(&sW[buf][jj][c], W + (size_t)(z0 + c) * ldw + j);
+      else sW[buf][jj][c] = 0.0;
+      if (j < J && x0 + c < nx) cp_async8(&sC[buf][jj][c], Ck + (size_t)j * nx + x0 + c);
+      else sC[buf][jj][c] = 0.0;
     }
+    cp_async_commit();
+  };
+  const int nblk = (J + 2 * BA_KM - 1) / (2 * BA_KM);
+  stage(0, 0);
+  for (int blk = 0; blk < nblk; ++blk) {
+    const int buf = blk & 1, jb = blk * 2 * BA_KM;
+    if (blk + 1 < nblk) stage(buf ^ 1, jb + 2 * BA_KM);
+    else cp_async_commit();
+    cp_async_wait<1>();
     __syncthreads();
     const int mend = min(BA_KM, (J - jb) / 2);
     for (int mm = 0; mm < mend; ++mm) {
       double wc[4], ws[4], ca[4], cb[4];
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
-        wc[a] = sW[2 * mm][ty + 16 * a];
-        ws[a] = sW[2 * mm + 1][ty + 16 * a];
+        wc[a] = sW[buf][2 * mm][ty + 16 * a];
+        ws[a] = sW[buf][2 * mm + 1][ty + 16 * a];
       }
 #pragma unroll
       for (int b = 0; b < 4; ++b) {
-        ca[b] = sC[2 * mm][tx + 16 * b];
-        cb[b] = sC[2 * mm + 1][tx + 16 * b];
+        ca[b] = sC[buf][2 * mm][tx + 16 * b];
+        cb[b] = sC[buf][2 * mm + 1][tx + 16 * b];
       }
 #pragma unroll
       for (int a = 0; a < 4; ++a)

@@ -200,6 +200,7 @@ struct Tf32GemmArgs {
   int KT;             // K tiles
   int NT;             // x tile images (128 rows of x) per array
   int MT;             // tiles of the other output dimension (j or z)
+  int NB_TILES;       // real 128-row tiles along N: x tiles (GEMM 1) or z tiles (GEMM 2)
   int narr;
   // EPI_COEF: C^T image out, [array][x-tile][KT2] tiles (rows x, k = j)
   float* c_hi;
@@ -214,23 +215,49 @@ struct Tf32GemmArgs {
 };
 
 constexpr int EPI_COEF = 0, EPI_APPLY = 1;
-constexpr int WS_NS = 3;                         // operand ring stages
-constexpr int WS_STAGE = 4 * TT_BYTES;           // A hi, A lo, B hi, B lo
 constexpr int WS_THREADS = 192;                  // producer, MMA, 4 epilogue warps
-constexpr uint32_t WS_TMEM_COLS = 256;           // two 128-column FP32 accumulators
-constexpr size_t WS_SMEM = (size_t)WS_NS * WS_STAGE + 1024;
-constexpr uint32_t WS_IDESC =
-    (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(128 >> 3) << 17) | ((uint32_t)(TT_M >> 4) << 24);
 
-template <int EPI>
-__device__ __forceinline__ void ws_tile(const Tf32GemmArgs& g, int t, int& k, int& xt, int& ot) {
-  ot = t % g.MT;              // j-tile (COEF) or z-tile (APPLY), fastest
-  xt = (t / g.MT) % g.NT;     // x tile image
-  k = t / (g.MT * g.NT);      // array
+// Output tiles are 128 x BN: BN = 256 takes two consecutive 128-row B tile
+// images per stage (the N dimension: x for GEMM 1, z for GEMM 2), so every
+// byte of A staged in shared memory feeds twice the MMA work.  Per stage:
+// A hi, A lo (16 KB each), B hi, B lo (BN/128 images each); the ring has as
+// many stages as fit (3 at BN = 128, 2 at 256); two BN-column FP32
+// accumulators in tensor memory.
+template <int BN>
+struct WsCfg {
+  static constexpr int NB = BN / TT_IMG_N;                  // B images per stage operand
+  static constexpr int STAGE = 2 * TT_BYTES + 2 * NB * TT_BYTES;
+  static constexpr int NS = BN == 128 ? 3 : 2;
+  static constexpr uint32_t TMEM_COLS = 2 * BN;
+  static constexpr size_t SMEM = (size_t)NS * STAGE + 1024;
+  static constexpr uint32_t IDESC =
+      (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TT_M >> 4) << 24);
+};
+
+// Tile t of a GEMM: array k, M tile (j-tile of GEMM 1 or x tile of GEMM 2)
+// and N group (x tiles or z tiles nb0 .. nb0 + NB - 1; those past the last
+// real tile repeat it and their columns are skipped).
+//   GEMM 1: N group fastest-varying after the j-tile: (k, N group, j-tile)
+//   GEMM 2: (k, x tile, N group), N group fastest
+template <int EPI, int NB>
+__device__ __forceinline__ void ws_tile(const Tf32GemmArgs& g, int t, int& k, int& mt, int& nb0) {
+  const int ngroups = (g.NB_TILES + NB - 1) / NB;
+  if (EPI == EPI_COEF) {
+    mt = t % g.MT;                   // j-tile, fastest
+    nb0 = ((t / g.MT) % ngroups) * NB;  // first x tile image of the group
+    k = t / (g.MT * ngroups);
+  } else {
+    nb0 = (t % ngroups) * NB;        // first z tile of the group, fastest
+    mt = (t / ngroups) % g.NT;       // x tile image
+    k = t / (ngroups * g.NT);
+  }
 }
 
-template <int EPI>
+template <int EPI, int BN>
 __global__ void __launch_bounds__(WS_THREADS, 1) tf32x3_gemm_ws(const __grid_constant__ Tf32GemmArgs g) {
+  using Cfg = WsCfg<BN>;
+  constexpr int WS_NS = Cfg::NS, WS_STAGE = Cfg::STAGE, NB = Cfg::NB;
+  constexpr uint32_t WS_TMEM_COLS = Cfg::TMEM_COLS, WS_IDESC = Cfg::IDESC;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* const smem =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
@@ -241,7 +268,8 @@ __global__ void __launch_bounds__(WS_THREADS, 1) tf32x3_gemm_ws(const __grid_con
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int KT = g.KT;
-  const int ntiles = g.narr * g.NT * g.MT;
+  const int ntiles = EPI == EPI_COEF ? g.narr * g.MT * ((g.NB_TILES + NB - 1) / NB)
+                                     : g.narr * g.NT * ((g.NB_TILES + NB - 1) / NB);
 
   if (tid == 0) {
     for (int s = 0; s < WS_NS; ++s) {
@@ -269,16 +297,16 @@ __global__ void __launch_bounds__(WS_THREADS, 1) tf32x3_gemm_ws(const __grid_con
       // producer: the operand tiles of every tile of this CTA, in order
       int q = 0;  // k-tiles issued so far
       for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        int k, xt, ot;
-        ws_tile<EPI>(g, t, k, xt, ot);
-        size_t a_off, b_off;
-        if (EPI == EPI_COEF) {
-          a_off = (size_t)ot * KT * TT_FLOATS;                           // Wt image [j-tile]
-          b_off = ((size_t)k * g.NT + xt) * KT * TT_FLOATS;              // G image [array][x-tile]
-        } else {
-          a_off = ((size_t)k * g.NT + xt) * KT * TT_FLOATS;              // C^T image [array][x-tile]
-          b_off = (size_t)ot * KT * TT_FLOATS;                           // W image [z-tile]
+        int k, mt, nb0;
+        ws_tile<EPI, NB>(g, t, k, mt, nb0);
+        size_t a_off, b_off[NB];
+        for (int i = 0; i < NB; ++i) {
+          const int nb = min(nb0 + i, g.NB_TILES - 1);  // past the last tile: repeat it (columns skipped)
+          b_off[i] = EPI == EPI_COEF ? ((size_t)k * g.NT + nb) * KT * TT_FLOATS   // G image [array][x-tile]
+                                     : (size_t)nb * KT * TT_FLOATS;                // W image [z-tile]
         }
+        a_off = EPI == EPI_COEF ? (size_t)mt * KT * TT_FLOATS                     // Wt image [j-tile]
+                                : ((size_t)k * g.NT + mt) * KT * TT_FLOATS;       // C^T image [array][x-tile]
         for (int kt = 0; kt < KT; ++kt, ++q) {
           const int s = q % WS_NS, u = q / WS_NS;
           if (u > 0) mbar_wait(&empty[s], (unsigned)((u - 1) & 1), g.err);
@@ -287,8 +315,10 @@ __global__ void __launch_bounds__(WS_THREADS, 1) tf32x3_gemm_ws(const __grid_con
           const size_t o = (size_t)kt * TT_FLOATS;
           bulk_g2s(st, g.a_hi + a_off + o, TT_BYTES, &full[s]);
           bulk_g2s(st + TT_BYTES, g.a_lo + a_off + o, TT_BYTES, &full[s]);
-          bulk_g2s(st + 2 * TT_BYTES, g.b_hi + b_off + o, TT_BYTES, &full[s]);
-          bulk_g2s(st + 3 * TT_BYTES, g.b_lo + b_off + o, TT_BYTES, &full[s]);
+          for (int i = 0; i < NB; ++i) {  // B hi images, then B lo images, each NB x 128 rows in a row
+            bulk_g2s(st + (2 + i) * TT_BYTES, g.b_hi + b_off[i] + o, TT_BYTES, &full[s]);
+            bulk_g2s(st + (2 + NB + i) * TT_BYTES, g.b_lo + b_off[i] + o, TT_BYTES, &full[s]);
+          }
         }
       }
     }
@@ -301,7 +331,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) tf32x3_gemm_ws(const __grid_con
         const int a = i & 1;
         if (i >= 2) mbar_wait(&acc_empty[a], (unsigned)(((i >> 1) - 1) & 1), g.err);
         tc_fence_after();
-        const uint32_t d = tmem + (uint32_t)(a * 128);
+        const uint32_t d = tmem + (uint32_t)(a * BN);
         for (int kt = 0; kt < KT; ++kt, ++q) {
           const int s = q % WS_NS, u = q / WS_NS;
           mbar_wait(&full[s], (unsigned)(u & 1), g.err);
@@ -311,7 +341,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) tf32x3_gemm_ws(const __grid_con
           for (int kk = 0; kk < TT_K / 8; ++kk) {
             const uint32_t off = (uint32_t)kk * 32u;  // 8 TF32 = 32 bytes along the swizzled row
             const uint64_t ah = sw128_desc(st + off), al = sw128_desc(st + TT_BYTES + off);
-            const uint64_t bh = sw128_desc(st + 2 * TT_BYTES + off), bl = sw128_desc(st + 3 * TT_BYTES + off);
+            const uint64_t bh = sw128_desc(st + 2 * TT_BYTES + off), bl = sw128_desc(st + (2 + NB) * TT_BYTES + off);
             umma_tf32(d, al, bh, WS_IDESC, (kt | kk) != 0 ? 1u : 0u);
             umma_tf32(d, ah, bl, WS_IDESC, 1u);
             umma_tf32(d, ah, bh, WS_IDESC, 1u);
@@ -327,20 +357,24 @@ __global__ void __launch_bounds__(WS_THREADS, 1) tf32x3_gemm_ws(const __grid_con
     const int r = 32 * quad + lane;
     int i = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
-      int k, xt, ot;
-      ws_tile<EPI>(g, t, k, xt, ot);
+      int k, mt, nb0;
+      ws_tile<EPI, NB>(g, t, k, mt, nb0);
       const int a = i & 1;
       mbar_wait(&acc_full[a], (unsigned)((i >> 1) & 1), g.err);
       __syncwarp();
       tc_fence_after();
-      const uint32_t src = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(a * 128);
+      const uint32_t src = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(a * BN);
 #pragma unroll 1
-      for (int cc = 0; cc < 128; cc += 32) {
+      for (int c0 = 0; c0 < BN; c0 += 32) {
+        const int nb = nb0 + c0 / TT_IMG_N;  // the N tile these 32 columns belong to
+        if (nb >= g.NB_TILES) break;         // a repeated tile past the end: skipped
+        const int cc = c0 % TT_IMG_N;        // columns within that tile
         uint32_t v[32];
-        tmem_ld32(src + (uint32_t)cc, v);
+        tmem_ld32(src + (uint32_t)c0, v);
         if (EPI == EPI_COEF) {
-          // row j = ot*128 + r; columns x = xt*128 + cc + i -> C^T image tile
-          // (xt, j/32), tile row cc + i, k-column j % 32 = lane
+          // row j = mt*128 + r; columns x = nb*128 + cc + c -> C^T image tile
+          // (nb, j/32), tile row cc + c, k-column j % 32 = lane
+          const int xt = nb, ot = mt;
           const int j = ot * TT_M + r;
           const size_t tb = (((size_t)k * g.NT + xt) * g.KT2 + (j >> 5)) * TT_FLOATS;
 #pragma unroll
@@ -352,8 +386,9 @@ __global__ void __launch_bounds__(WS_THREADS, 1) tf32x3_gemm_ws(const __grid_con
             g.c_lo[tb + o] = lo;
           }
         } else {
-          // row x = xt*128 + r; columns z = ot*128 + cc + c: G_k[z, x] -= D
+          // row x = mt*128 + r; columns z = nb*128 + cc + c: G_k[z, x] -= D
           // (z < nz; the padded rows of a last partial z tile are skipped)
+          const int xt = mt, ot = nb;
           const int x = xt * TT_IMG_N + r;
           const int z0 = ot * TT_M + cc;
           if (x < g.nx && z0 < g.nz) {
@@ -398,10 +433,37 @@ int tf32_zpad(int nz) { return ((nz + TT_M - 1) / TT_M) * TT_M; }
 size_t tf32_tile_floats() { return TT_FLOATS; }
 
 cudaError_t prepare_tf32() {
-  cudaError_t e =
-      cudaFuncSetAttribute(tf32x3_gemm_ws<EPI_COEF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WS_SMEM);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(tf32x3_gemm_ws<EPI_APPLY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WS_SMEM);
+  cudaError_t e = cudaFuncSetAttribute(tf32x3_gemm_ws<EPI_COEF, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)WsCfg<128>::SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(tf32x3_gemm_ws<EPI_APPLY, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)WsCfg<128>::SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(tf32x3_gemm_ws<EPI_COEF, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)WsCfg<256>::SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(tf32x3_gemm_ws<EPI_APPLY, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)WsCfg<256>::SMEM);
+  return e;
+}
+
+// 128 x 256 tiles halve the A operand traffic per MMA but halve the tile
+// count too; they are used when the GEMM still has at least 10 waves of
+// tiles over the SMs.  Measured on B200, TF32 band stage: 2.58 against 2.90
+// ms at 2048 x 4096 and 16.6 against 19.7 ms at 4096 x 8192, but 0.485
+// against 0.464 ms at 1024 x 2048, where the wider tiles leave GEMM 1 3.4
+// waves and GEMM 2 9.1.  Both widths give the same bits: each output's MMAs
+// and their order are the same.
+template <int EPI>
+static cudaError_t launch_gemm(const Tf32GemmArgs& g, int ntiles_m_side, int sms, cudaStream_t s) {
+  const int n256 = g.narr * ntiles_m_side * ((g.NB_TILES + 1) / 2);
+  if (n256 >= 10 * sms) {
+    tf32x3_gemm_ws<EPI, 256><<<std::min(n256, sms), WS_THREADS, WsCfg<256>::SMEM, s>>>(g);
+  } else {
+    const int n128 = g.narr * ntiles_m_side * g.NB_TILES;
+    tf32x3_gemm_ws<EPI, 128><<<std::min(n128, sms), WS_THREADS, WsCfg<128>::SMEM, s>>>(g);
+  }
+  return cudaGetLastError();
 }
 
 cudaError_t launch_tf32_w_images(const double* W, int ldw, int J, int nz, const Tf32BandImages& b, cudaStream_t s) {
@@ -430,6 +492,7 @@ cudaError_t launch_band_tf32(const ArrayList& arrs, int narr, const Tf32BandImag
   g1.KT = KT1;
   g1.NT = NT;
   g1.MT = MT1;
+  g1.NB_TILES = NT;  // N = x
   g1.narr = narr;
   g1.c_hi = w.ch;
   g1.c_lo = w.cl;
@@ -439,9 +502,7 @@ cudaError_t launch_band_tf32(const ArrayList& arrs, int narr, const Tf32BandImag
   g1.nx = nx;
   g1.nz = nz;
   g1.err = err;
-  const int t1 = narr * NT * MT1;
-  tf32x3_gemm_ws<EPI_COEF><<<std::min(t1, sms), WS_THREADS, WS_SMEM, s>>>(g1);
-  e = cudaGetLastError();
+  e = launch_gemm<EPI_COEF>(g1, MT1, sms, s);
   if (e != cudaSuccess) return e;
   Tf32GemmArgs g2 = g1;
   g2.a_hi = w.ch;   // C^T image [array][x-tile][KT2]
@@ -450,9 +511,8 @@ cudaError_t launch_band_tf32(const ArrayList& arrs, int narr, const Tf32BandImag
   g2.b_lo = b.a2l;
   g2.KT = KT2;
   g2.MT = MT2;
-  const int t2 = narr * NT * MT2;
-  tf32x3_gemm_ws<EPI_APPLY><<<std::min(t2, sms), WS_THREADS, WS_SMEM, s>>>(g2);
-  return cudaGetLastError();
+  g2.NB_TILES = MT2;  // N = z
+  return launch_gemm<EPI_APPLY>(g2, NT, sms, s);
 }
 
 }  // namespace ymkh
