@@ -334,6 +334,7 @@ def main() -> int:
     ap.add_argument("--filter-error-control", action="store_true",
                     help="the error leg as a control: FP64 filter against FP64 filter with nA scaled by 1+2^-52 at the start")
     ap.add_argument("--batched-runs", type=int, default=64, help="runs in the batched-vs-plain leg (0: skip)")
+    ap.add_argument("--batched-steps", type=int, default=2000, help="steps per run in the batched-vs-plain leg")
     ap.add_argument("--ref-sweep-runs", type=int, default=64,
                     help="--impl reference: also time the reference's kernels over the uneven sweep (0: skip)")
     ap.add_argument("--batch-by-size", action="store_true",
@@ -450,7 +451,7 @@ def main() -> int:
         line["filter_error"] = filter_error(args, dev, args.filter_error_steps, args.filter_error_runs,
                                             control=args.filter_error_control)
     if world == 1 and args.batched_runs > 0:
-        line["batched"] = batched_rate(args, dev, args.batched_runs)
+        line["batched"] = batched_rate(args, dev, args.batched_runs, args.batched_steps)
     if world == 1 and args.batch_by_size:
         line["batch_by_size"] = batch_by_size(dev)
     if world == 1 and args.served_seconds > 0:
@@ -585,12 +586,19 @@ def batch_by_size(dev) -> list:
     return out
 
 
-def batched_rate(args, dev, nruns: int) -> dict:
-    """Uneven sweep of `nruns` runs (seed 1; NZ 128..1024, NX 256..2048):
-    aggregate cell-steps/s of the batched form (one FCT and one Maxwell
-    launch per step over every run's tiles, CUDA graphs) against the same
-    runs stepped one after another through the plain single-run step, from
-    the same state; the two final states are compared run by run."""
+def batched_rate(args, dev, nruns: int, steps: int, check: int = 100) -> dict:
+    """Config 2: the uneven sweep of `nruns` runs (seed 1; NZ 128..1024, NX
+    256..2048) for `steps` steps each, with the energy checked every `check`
+    steps and the reference's halt rule applied (NaN/Inf or E/E0 above the
+    threshold, ymgpu2d/main_ym.cu:467-474): aggregate cell-steps/s of the
+    batched form (one FCT and one Maxwell launch per step over every run's
+    tiles, CUDA graphs; halted runs leave the batch) against the same runs
+    stepped one after another through the plain single-run step, from the
+    same state, timed with CUDA events on one stream around the whole pass
+    (energy checks included).  Final states and halt steps of the two passes
+    are compared run by run."""
+    import math
+
     import torch
 
     from kh_simulations_b200.batch import KHBatch
@@ -601,17 +609,30 @@ def batched_rate(args, dev, nruns: int) -> dict:
     runs = [KHRun(c, device=dev) for c in uneven_sweep(1, nruns, SWEEP_BASE)]
     for r in runs:
         r.init(stream=stream)
+        r.E0 = r.energy(stream)
         r.step(4, stream)  # warm-up: graphs captured, current buffer back to 0
     torch.cuda.synchronize(dev)
     s0 = [r.state.clone() for r in runs]
-    cells = sum(r.d.nx * r.d.nz for r in runs)
-    k = max(2, args.steps - args.steps % 2)
+
+    def halted(r):
+        e = r.energy(stream)
+        return not math.isfinite(e) or e / r.E0 > r.d.energy_thresh
 
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    plain_steps, plain_state = [], []
+    cs_plain = 0
     e0.record(stream)
     for r in runs:
-        r.step(k, stream)
+        done = 0
+        while done < steps:
+            k = min(check, steps - done)
+            r.step(k, stream)
+            done += k
+            if halted(r):
+                break
+        plain_steps.append(done)
+        cs_plain += done * r.d.nx * r.d.nz
     e1.record(stream)
     e1.synchronize()
     ms_plain = e0.elapsed_time(e1)
@@ -628,22 +649,40 @@ def batched_rate(args, dev, nruns: int) -> dict:
     for r, s in zip(runs, s0):
         r.set_state(s)
     torch.cuda.synchronize(dev)
+    live = list(runs)
+    batch_steps = {id(r): 0 for r in runs}
+    cs_batch = 0
     e0.record(stream)
-    batch.step(k, stream)
+    done = 0
+    while done < steps and live:
+        k = min(check, steps - done)
+        batch.step(k, stream)
+        done += k
+        for r in list(live):
+            batch_steps[id(r)] = done
+            cs_batch += k * r.d.nx * r.d.nz
+            if halted(r):
+                batch.remove(r)
+                live.remove(r)
     e1.record(stream)
     e1.synchronize()
     ms_batch = e0.elapsed_time(e1)
     dev_max = max(_rel_l2_max(r.state, p) for r, p in zip(runs, plain_state))
+    same_halts = all(batch_steps[id(r)] == n for r, n in zip(runs, plain_steps))
     batch.close()
+    cells = sum(r.d.nx * r.d.nz for r in runs)
     for r in runs:
         r.close()
     del runs, s0, plain_state
     torch.cuda.empty_cache()
-    plain = cells * k / (ms_plain / 1e3)
-    batched = cells * k / (ms_batch / 1e3)
-    return {"workload": f"uneven sweep, {nruns} runs (seed 1), {cells} cells, {k} steps",
+    plain = cs_plain / (ms_plain / 1e3)
+    batched = cs_batch / (ms_batch / 1e3)
+    return {"workload": f"config 2: uneven sweep, {nruns} runs (seed 1), {cells} cells, {steps} steps, "
+                        f"energy and halt rule every {check} steps",
             "batched_cell_steps_per_s": batched, "plain_cell_steps_per_s": plain, "batched_over_plain": batched / plain,
-            "max_rel_l2_batched_vs_plain": dev_max, "unit": "cell-steps/s", "timing": "CUDA events, one stream"}
+            "halted_runs": sum(n < steps for n in plain_steps), "same_halt_steps": same_halts,
+            "max_rel_l2_batched_vs_plain": dev_max, "unit": "cell-steps/s",
+            "timing": "CUDA events, one stream, around each whole pass"}
 
 
 def _served_pass(dev, seconds, drain, step_scale, engine, large_cells):
