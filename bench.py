@@ -697,12 +697,26 @@ def _served_pass(dev, seconds, drain, step_scale, engine, large_cells):
         return poisson_mix(3, 20.0, seconds, 128 * 256, 2048 * 4096, max(1, 2000 // step_scale),
                            max(2, 20000 // step_scale), SWEEP_BASE, keep_third=True, filter_engine=engine)
 
+    import torch
+
     srv = KHServer(150 << 30, device=dev, chunk=50, large_cells=large_cells)
-    served = srv.serve(mix(), deadline=seconds + drain)
-    seq = srv.serve_sequential(mix(), deadline=seconds + drain)
+    gpu = dev.index if dev.index is not None else 0
+
+    def one(fn):
+        # each pass starts from an empty allocator cache, with its clocks sampled
+        torch.cuda.synchronize(dev)
+        torch.cuda.empty_cache()
+        cs = ClockSampler(gpu)
+        cs.start()
+        rep = fn(mix(), deadline=seconds + drain)
+        return rep, cs.stop()
+
+    served, clk_a = one(srv.serve)
+    seq, clk_b = one(srv.serve_sequential)
     a, b = served.summary(), seq.summary()
+    a["clocks"], b["clocks"] = clk_a, clk_b
     keys = ("requests", "completed", "unfinished", "halted", "makespan_s", "cell_steps", "cell_steps_per_s",
-            "p50_latency_s", "p99_latency_s")
+            "p50_latency_s", "p99_latency_s", "clocks")
     # measured Amdahl bound: service time of the sequential pass split into
     # runs below / at or above large_cells; batching can at best remove the
     # former, since a large run fills the GPU alone

@@ -194,6 +194,28 @@ class KHServer:
             out.append((req, fp))
         return out
 
+    def _halted_many(self, runs, stream) -> list:
+        """The reference's halt rule for several runs, with their energies
+        reduced on the device and read back by one synchronisation (the
+        error words of the batch's kernels are checked by the caller)."""
+        import ctypes as C
+
+        import torch
+
+        if not self.check_energy or not runs:
+            return [False] * len(runs)
+        out = torch.empty(len(runs), dtype=torch.float64, device=runs[0].device)
+        lib = runs[0].lib
+        for i, run in enumerate(runs):
+            rc = lib.ymkh_energy_async(run.ctx, C.c_void_p(out.data_ptr() + 8 * i), C.c_void_p(stream.cuda_stream))
+            if rc:
+                from ._lib import check
+
+                check(rc, "ymkh_energy_async")
+        stream.synchronize()
+        es = out.cpu().tolist()
+        return [not math.isfinite(e) or e / r.E0 > r.d.energy_thresh for e, r in zip(es, runs)]
+
     def _halted(self, run, stream) -> bool:
         if not self.check_energy:
             return False
@@ -271,10 +293,13 @@ class KHServer:
                 cell_steps += kl * head[0].cells
             t = self.clock() - t0
             done, keep = [], []
-            for a in small:
+            if ks:
+                batch.check(s_small)  # bounded in-kernel waits of the batch's step
+            halts = self._halted_many([a[1] for a in small], s_small) if ks else [False] * len(small)
+            for a, h in zip(small, halts):
                 req, run, fp, rem = a
                 status = ("done" if rem <= 0 else "cancelled" if req.cancel_at <= t
-                          else "halted" if ks and self._halted(run, s_small) else None)
+                          else "halted" if h else None)
                 if status:
                     batch.remove(run)
                     done.append((a, status))
