@@ -324,6 +324,7 @@ def main() -> int:
     ap.add_argument("--filter", choices=["ref", "keep"], default="ref")
     ap.add_argument("--filter-engine", choices=["dft", "tf32x3"], default="dft",
                     help="band filter of the main run: FP64 sums or 3-pass TF32 on the tensor cores")
+    ap.add_argument("--no-config0", action="store_true", help="skip the config-0 leg (256 x 512, keep |k| <= 85)")
     ap.add_argument("--no-filter-keep", action="store_true",
                     help="skip the config-1-as-stated leg (filter on at the workload size, both engines)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -456,7 +457,7 @@ def main() -> int:
         line["batch_by_size"] = batch_by_size(dev)
     if world == 1 and args.served_seconds > 0:
         line["served"] = served_rate(args, dev, args.served_seconds)
-    if world == 1:
+    if world == 1 and not args.no_config0:
         line["config0"] = config0_rate(dev)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_oracle_rate(args.workload, 1, min_seconds=10.0)
