@@ -34,6 +34,11 @@ from pathlib import Path
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
+# The served leg creates and frees about a thousand runs of mixed sizes; with
+# expandable segments torch's caching allocator maps device memory in pages
+# and can return freed pages, so pieces of retired runs' buffers do not keep
+# whole segments reserved (set before torch first touches the device).
+os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "expandable_segments:True")
 
 WORKLOADS = {
     # name: (NX shear, NZ periodic)

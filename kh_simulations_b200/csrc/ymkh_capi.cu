@@ -208,7 +208,10 @@ int setup_params(ymkh_ctx* c, const ymkh_params* p) {
   } else if (nb) {
     CK(cudaMalloc(&c->coef, 21 * maxJ * (size_t)c->nx * sizeof(double)), "cudaMalloc band coefficients");
   }
-  CK(cudaDeviceSynchronize(), "twiddle setup");
+  // the twiddle tables and images are built on the legacy default stream:
+  // wait for that stream only, not for other streams' work in flight (a
+  // server creates runs while others step)
+  CK(cudaStreamSynchronize(0), "twiddle setup");
   return 0;
 }
 

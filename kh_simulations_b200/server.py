@@ -146,24 +146,35 @@ class KHServer:
         self.large_cells = int(large_cells)
 
     # ---------------------------------------------------------------- helpers
-    def _start_run(self, req: KHRequest, stream=None):
+    def _start_run(self, req: KHRequest, stream=None, must: bool = True):
+        """A new run for `req`, initialised on `stream`.  If the device has
+        no room for it (the budget counts live runs, but the caching
+        allocator may still hold pieces of retired ones), cached memory is
+        released and the creation retried once; if that fails too, None is
+        returned when `must` is false (the caller retries after retiring
+        runs), else the error is raised."""
         import torch
 
         from ._lib import YMKHError
         from .run import KHRun
 
+        def create():
+            try:
+                return KHRun(req.cfg, device=self.device, graph_steps=self.graph_steps)
+            except (YMKHError, torch.OutOfMemoryError):
+                if must and attempt == 1:
+                    raise
+                return None
+
         run = None
-        try:
-            run = KHRun(req.cfg, device=self.device, graph_steps=self.graph_steps)
-        except (YMKHError, torch.OutOfMemoryError):
-            pass
-        if run is None:
-            # the budget counts live runs, but torch's caching allocator may
-            # still hold the buffers of retired ones (and of the failed
-            # attempt): release them and retry once
+        for attempt in (0, 1):
+            run = create()
+            if run is not None:
+                break
             torch.cuda.synchronize(self.device)
             torch.cuda.empty_cache()
-            run = KHRun(req.cfg, device=self.device, graph_steps=self.graph_steps)
+        if run is None:
+            return None
         run.init(stream=stream)
         run.E0 = run.energy(stream)
         return run
@@ -254,6 +265,7 @@ class KHServer:
         used = 0
         cell_steps = 0
         t0 = self.clock()
+        self.deferred = 0
         first = pending[0].arrival if pending else 0.0
         while pending or small or large:
             now = self.clock() - t0
@@ -274,8 +286,17 @@ class KHServer:
                 head[1].step(kl, s_large)
             # admissions while the device works; new runs start on their own stream
             admitted = []
-            for req, fp in self.admit_order(pending, now, used):
-                run = self._start_run(req, s_admit)
+            cand = self.admit_order(pending, now, used)
+            for i, (req, fp) in enumerate(cand):
+                # with runs resident, a creation that finds no room waits,
+                # with the candidates after it, at the head of the queue for
+                # runs to retire
+                run = self._start_run(req, s_admit, must=not (small or large or admitted))
+                if run is None:
+                    for r, _ in reversed(cand[i:]):
+                        pending.appendleft(r)
+                    self.deferred += 1
+                    break
                 req.admitted = self.clock() - t0
                 req.status = "running"
                 admitted.append([req, run, fp, req.steps])
@@ -334,8 +355,8 @@ class KHServer:
         makespan = end - first
         p50, p99 = _percentiles(requests)
         return ServeReport(requests, makespan, cell_steps, p50, p99, "batched",
-                           {"large_cells": self.large_cells, "unfinished": sum(r.status == "unfinished"
-                                                                              for r in requests)})
+                           {"large_cells": self.large_cells, "deferred_admissions": self.deferred,
+                            "unfinished": sum(r.status == "unfinished" for r in requests)})
 
     def serve_sequential(self, requests: list, deadline: float = math.inf) -> ServeReport:
         """The same requests one by one through the plain single-run step, in
