@@ -85,6 +85,13 @@ constexpr size_t fct_smem_bytes(int nst) {
 }
 
 
+// One TMA bulk row copy of a stage (the table in fct_fused_kernel).
+struct RowCopy {
+  const double* base;
+  const double* base0;
+  int dst, kind, len1, pad_;
+};
+
 // Per-thread z-pipeline state for the three swept variables of one half
 // (H = 0: n, px, pz; H = 1: Q1, Q2, Q3) of one beam.
 struct ZPipe {
@@ -107,6 +114,7 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
 
   __shared__ RunDesc rd;
   __shared__ int s_run;
+  __shared__ RowCopy cpt[40];
   const State& st = rd.in;
   const State& out = rd.out;
   const StepParams& p = rd.p;
@@ -175,33 +183,37 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
     for (int i = tid; i < 2 * 2 * W; i += NT) wk[(size_t)(i / (2 * W)) * WB_SIZE * W + WB_SZ * W + i % (2 * W)] = 0.0;
     __syncthreads();
 
-    // bulk rows: this thread's row copy for the item (array a of the stage,
-    // lane-major over the warps): source array, stage slot, which row (0: z,
-    // 1: z-1, 2: z+1) and the split at the periodic wrap
-    const double* cp_base = nullptr;
-    int cp_dst = 0, cp_kind = 0, cp_x1 = 0, cp_len1 = W;
-    if (bulk) {
-      const int a = (tid & 31) * (NT / 32) + (tid >> 5);
-      if (a < 33 + (warm ? 4 : 0)) {
-        if (a < 12) {
-          cp_base = a < 6 ? st.a[a] : st.b[a - 6];
-          cp_dst = ST_FL + a;
-        } else if (a < 33) {
-          const int kind = (a - 12) / 3, c = (a - 12) - kind * 3;  // EX, BY, BYM, EZ, EZM, AZ, AZM
-          cp_base = (kind == 0) ? st.f[EX1 + c] : (kind <= 2) ? st.f[BY1 + c] : (kind <= 4) ? st.f[EZ1 + c] : st.f[AZ1 + c];
-          cp_dst = ST_EX + (a - 12);
-          cp_kind = (kind == 2 || kind == 4 || kind == 6) ? 1 : 0;
-        } else {
-          const int w = a - 33;  // NZP A, NZP B, NZM A, NZM B
-          cp_base = (w & 1) ? st.b[FN] : st.a[FN];
-          cp_dst = ST_NZP + w;
-          cp_kind = (w >> 1) ? 1 : 2;
-        }
-        int x = (x0 - 4) % nx;
-        cp_x1 = x < 0 ? x + nx : x;
-        cp_len1 = min(W, nx - cp_x1);
+    // bulk rows: the row copies of the item, one per array of the stage
+    // (source array at the strip's first column and at column 0 for the part
+    // past the periodic wrap, stage slot offset, which row, length before the
+    // wrap) in a shared table read by the issuing thread
+    if (bulk && tid < 33 + (warm ? 4 : 0)) {
+      const int a = tid;
+      const double* base;
+      int dst, kind_row = 0;
+      if (a < 12) {
+        base = a < 6 ? st.a[a] : st.b[a - 6];
+        dst = ST_FL + a;
+      } else if (a < 33) {
+        const int kind = (a - 12) / 3, c = (a - 12) - kind * 3;  // EX, BY, BYM, EZ, EZM, AZ, AZM
+        base = (kind == 0) ? st.f[EX1 + c] : (kind <= 2) ? st.f[BY1 + c] : (kind <= 4) ? st.f[EZ1 + c] : st.f[AZ1 + c];
+        dst = ST_EX + (a - 12);
+        kind_row = (kind == 2 || kind == 4 || kind == 6) ? 1 : 0;
+      } else {
+        const int w = a - 33;  // NZP A, NZP B, NZM A, NZM B
+        base = (w & 1) ? st.b[FN] : st.a[FN];
+        dst = ST_NZP + w;
+        kind_row = (w >> 1) ? 1 : 2;
       }
+      int x = (x0 - 4) % nx;
+      x = x < 0 ? x + nx : x;
+      cpt[a].base = base + x;
+      cpt[a].base0 = base;
+      cpt[a].dst = dst;
+      cpt[a].kind = kind_row;
+      cpt[a].len1 = min(W, nx - x);
     }
+    __syncthreads();
 
     auto issue_row = [&](int r) {
       const int s = (int)(issued % NST);
@@ -218,13 +230,17 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
         // and the phase cannot complete before that arrival.  The copy's
         // array, slot and wrap split are fixed per item (cp_*).
         if (tid == 0) mbar_expect_tx(&bars[s], (unsigned)(narr * W * 8));
-        if (cp_base && dbg_ok(zr >= 0 && zr < nz && zm >= 0 && zm < nz && zp >= 0 && zp < nz && cp_x1 >= 0 &&
-                                  cp_len1 > 0 && cp_x1 + cp_len1 <= nx && W - cp_len1 <= nx && cp_dst >= 0 &&
-                                  cp_dst < ST_SIZE, T.err)) {
-          const size_t off = cp_kind == 0 ? ro : (cp_kind == 1 ? rom : rop);
-          double* const dst = sb + cp_dst * W;
-          bulk_g2s(dst, cp_base + off + cp_x1, (unsigned)cp_len1 * 8u, &bars[s]);
-          if (cp_len1 < W) bulk_g2s(dst + cp_len1, cp_base + off, (unsigned)(W - cp_len1) * 8u, &bars[s]);
+        const int ca = (tid & 31) * (NT / 32) + (tid >> 5);  // lane-major over the warps
+        if (ca < narr) {
+          const RowCopy& c = cpt[ca];
+          const int len1 = c.len1;
+          if (dbg_ok(zr >= 0 && zr < nz && zm >= 0 && zm < nz && zp >= 0 && zp < nz && len1 > 0 && W - len1 <= nx &&
+                         c.dst >= 0 && c.dst < ST_SIZE, T.err)) {
+            const size_t off = c.kind == 0 ? ro : (c.kind == 1 ? rom : rop);
+            double* const dst = sb + c.dst * W;
+            bulk_g2s(dst, c.base + off, (unsigned)len1 * 8u, &bars[s]);
+            if (len1 < W) bulk_g2s(dst + len1, c.base0 + off, (unsigned)(W - len1) * 8u, &bars[s]);
+          }
         }
       } else {
         const bool rows_ok = dbg_ok(zr >= 0 && zr < nz && zm >= 0 && zm < nz && zp >= 0 && zp < nz, T.err);
@@ -292,6 +308,7 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
       // (FCT_Sweeps.cu:88-98); half 0 also forms the px source at sp
       // (YM_Fluid.cu:43-66, 71-80).
       double vz_own, ux_own, mu_if = 0.0, sx = 0.0;
+      double Fo[3] = {0.0, 0.0, 0.0}, Do[3] = {0.0, 0.0, 0.0};  // this thread's interface fluxes
       {
         const double n0 = max_sel(fl[FN * W + sp], 0.05);
         ux_own = fl[FPX * W + sp] / n0;
@@ -306,8 +323,10 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
           for (int j = 0; j < 3; ++j) {
             const int k = k0 + j;
             const double v0 = fl[k * W + sp], v1 = fl[k * W + sp + 1];
-            wb[(WB_F + k) * W + sp] = 0.5 * e * (v0 + v1);
-            wb[(WB_D + k) * W + sp] = nu * (v1 - v0);
+            Fo[j] = 0.5 * e * (v0 + v1);
+            Do[j] = nu * (v1 - v0);
+            wb[(WB_F + k) * W + sp] = Fo[j];
+            wb[(WB_D + k) * W + sp] = Do[j];
           }
         }
         if (half == 0 && t >= 1 && t < TB - 1) {
@@ -336,31 +355,36 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
       beam_bar(grp, TB);
 
       // ---- B: lorhot / lnrhot at sp (FCT_Sweeps.cu:102-103), t in [1, TB-1).
+      double Lo[3] = {0.0, 0.0, 0.0}, Ln[3] = {0.0, 0.0, 0.0};  // this thread's lorhot, lnrhot
       if (t >= 1 && t < TB - 1) {
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
           const int k = k0 + j;
           const double v0 = fl[k * W + sp];
-          const double fd = wb[(WB_F + k) * W + sp] - wb[(WB_F + k) * W + sp - 1];
-          const double dd = wb[(WB_D + k) * W + sp] - wb[(WB_D + k) * W + sp - 1];
+          const double fd = Fo[j] - wb[(WB_F + k) * W + sp - 1];
+          const double dd = Do[j] - wb[(WB_D + k) * W + sp - 1];
           const double lo = (k == FPX) ? v0 + dt * sx - fd : v0 - fd;
+          Lo[j] = lo;
+          Ln[j] = lo + dd;
           wb[(WB_LOR + k) * W + sp] = lo;
-          wb[(WB_LNR + k) * W + sp] = lo + dd;
+          wb[(WB_LNR + k) * W + sp] = Ln[j];
         }
       }
       beam_bar(grp, TB);
 
       // ---- C: antidiffusive flux and limiter at interface sp+1/2
       // (FCT_Sweeps.cu:139-160), t in [2, TB-3).
+      double Fl[3] = {0.0, 0.0, 0.0};  // this thread's limited flux
       if (t >= 2 && t < TB - 3) {
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
           const int k = k0 + j;
           const double* lor = wb + (WB_LOR + k) * W;
           const double* lnr = wb + (WB_LNR + k) * W;
-          const double fad = mu_if * (lor[sp + 1] - lor[sp]);
-          wb[(WB_FLIM + k) * W + sp] =
-              fct_limit_sel(fad, lnr[sp] - lnr[sp - 1], lnr[sp + 1] - lnr[sp], lnr[sp + 2] - lnr[sp + 1]);
+          const double l1 = lnr[sp + 1];
+          const double fad = mu_if * (lor[sp + 1] - Lo[j]);
+          Fl[j] = fct_limit_sel(fad, Ln[j] - lnr[sp - 1], l1 - Ln[j], lnr[sp + 2] - l1);
+          wb[(WB_FLIM + k) * W + sp] = Fl[j];
         }
       }
       beam_bar(grp, TB);
@@ -371,7 +395,7 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
           const int k = k0 + j;
-          Vx[j] = wb[(WB_LNR + k) * W + sp] - (wb[(WB_FLIM + k) * W + sp] - wb[(WB_FLIM + k) * W + sp - 1]);
+          Vx[j] = Ln[j] - (Fl[j] - wb[(WB_FLIM + k) * W + sp - 1]);
         }
         const double vz = vz_own;
         const double q1 = fl[FQ1 * W + sp], q2 = fl[FQ2 * W + sp], q3 = fl[FQ3 * W + sp];
