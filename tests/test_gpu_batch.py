@@ -168,6 +168,36 @@ def test_server_large_runs_alone_equal_sequential(cuda):
     assert rep.extra["unfinished"] == 0
 
 
+def test_server_defers_an_admission_without_room(cuda, monkeypatch):
+    """A run creation that finds no device room while other runs are
+    resident puts the request (and those after it) back at the head of the
+    queue until runs retire; every request still completes, equal to its
+    sequential run.  The lack of room is simulated on the host: the server's
+    creation call reports it once."""
+    from kh_simulations_b200.server import KHRequest, KHServer
+
+    reqs_a = [KHRequest(i, _cfg(t), 16 + 4 * i, arrival=0.0) for i, (t, _) in enumerate(MIX[:4])]
+    reqs_b = [KHRequest(i, _cfg(t), 16 + 4 * i, arrival=0.0) for i, (t, _) in enumerate(MIX[:4])]
+    srv = KHServer(budget_bytes=2 << 30, chunk=8, keep_state=True)
+    real = KHServer._start_run
+    failed = []
+
+    def flaky(self, req, stream=None, must=True):
+        if not must and req.rid == 2 and not failed:
+            failed.append(req.rid)
+            return None  # as if creation found no room
+        return real(self, req, stream, must)
+
+    monkeypatch.setattr(KHServer, "_start_run", flaky)
+    rep = srv.serve(reqs_a)
+    monkeypatch.setattr(KHServer, "_start_run", real)
+    srv.serve_sequential(reqs_b)
+    assert failed == [2] and rep.extra["deferred_admissions"] == 1
+    for a, s in zip(sorted(reqs_a, key=lambda r: r.rid), sorted(reqs_b, key=lambda r: r.rid)):
+        assert a.status == s.status == "done", (a.rid, a.status)
+        assert np.array_equal(a.state, s.state), a.rid
+
+
 def test_autotune_runs_and_keeps_results(cuda, tmp_path, monkeypatch):
     import kh_simulations_b200.autotune as at
     from kh_simulations_b200.run import KHRun
