@@ -85,6 +85,15 @@ constexpr size_t fct_smem_bytes(int nst) {
 }
 
 
+// The half of a thread group as a compile-time constant: the row loop is
+// compiled once per half, with the swept variables' shared-memory offsets,
+// which variables carry z-sources and which source each half forms fixed
+// (1.0% faster at 4096 x 8192 than one loop that branches on the half).
+template <int V>
+struct HalfC {
+  static constexpr int value = V;
+};
+
 // One TMA bulk row copy of a stage (the table in fct_fused_kernel).
 struct RowCopy {
   const double* base;
@@ -125,7 +134,6 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
   const int t = tid - grp * TB;
   const int sp = t + 1;         // this thread's stage position
   double* const wb = wk + (size_t)beam * WB_SIZE * W;
-  const int k0 = 3 * half;      // first swept variable of this half
 
   if (tid == 0) {
     for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
@@ -278,201 +286,208 @@ __global__ void __launch_bounds__(4 * TB, (TB >= 128 ? 1 : 2))
       if (r_first + k <= r_last) issue_row(r_first + k);
       else if (!bulk) cp_async_commit();
 
-    ZPipe zp;
+    // the piece's rows, for this thread's half (a compile-time constant here)
+    auto rows = [&](auto HC) {
+      constexpr int half = decltype(HC)::value;
+      constexpr int k0 = 3 * half;  // first swept variable of this half
+      ZPipe zp;
 #pragma unroll
-    for (int j = 0; j < 3; ++j)
-      zp.V1[j] = zp.f1[j] = zp.d1[j] = zp.L2[j] = zp.N4[j] = zp.N3[j] = zp.N2[j] = zp.A2[j] = zp.F3[j] = zp.S1[j] = 0.0;
-    zp.U1 = zp.mu1 = 0.0;
-    const int x_own = x0 - 4 + sp;
-    const bool zthread = (t >= 3) && (t < TB - 3);  // owns an output column
-    const bool owner = zthread && (x_own < nx);
+      for (int j = 0; j < 3; ++j)
+        zp.V1[j] = zp.f1[j] = zp.d1[j] = zp.L2[j] = zp.N4[j] = zp.N3[j] = zp.N2[j] = zp.A2[j] = zp.F3[j] = zp.S1[j] = 0.0;
+      zp.U1 = zp.mu1 = 0.0;
+      const int x_own = x0 - 4 + sp;
+      const bool zthread = (t >= 3) && (t < TB - 3);  // owns an output column
+      const bool owner = zthread && (x_own < nx);
 
-    for (int r = r_first; r <= r_last; ++r) {
-      const int s = (int)(consumed % NST);
-      if (bulk) {  // one thread polls the stage's mbarrier; the CTA barrier below
-        // releases the others after it (no spinning by every thread)
-        if (tid == 0) mbar_wait(&bars[s], (phase_bits >> s) & 1u, T.err);
-        phase_bits ^= 1u << s;
-      } else {
-        cp_async_wait<NST - 2>();
-      }
-      __syncthreads();  // row r staged for everyone; the previous row's stage is free
-      ++consumed;
-      if (r + NST - 1 <= r_last) issue_row(r + NST - 1);
-      else if (!bulk) cp_async_commit();
-      const double* sb = stage + (size_t)s * ST_SIZE * W;
-      const double* fl = sb + (size_t)(ST_FL + beam * 6) * W;
+      for (int r = r_first; r <= r_last; ++r) {
+        const int s = (int)(consumed % NST);
+        if (bulk) {  // one thread polls the stage's mbarrier; the CTA barrier below
+          // releases the others after it (no spinning by every thread)
+          if (tid == 0) mbar_wait(&bars[s], (phase_bits >> s) & 1u, T.err);
+          phase_bits ^= 1u << s;
+        } else {
+          cp_async_wait<NST - 2>();
+        }
+        __syncthreads();  // row r staged for everyone; the previous row's stage is free
+        ++consumed;
+        if (r + NST - 1 <= r_last) issue_row(r + NST - 1);
+        else if (!bulk) cp_async_commit();
+        const double* sb = stage + (size_t)s * ST_SIZE * W;
+        const double* fl = sb + (size_t)(ST_FL + beam * 6) * W;
 
-      // ---- A: velocities at sp, sp+1 (YM_Fluid.cu:3-11); interface sp+1/2:
-      // eps, nu, mu and the low-order fluxes of this half's variables
-      // (FCT_Sweeps.cu:88-98); half 0 also forms the px source at sp
-      // (YM_Fluid.cu:43-66, 71-80).
-      double vz_own, ux_own, mu_if = 0.0, sx = 0.0;
-      double Fo[3] = {0.0, 0.0, 0.0}, Do[3] = {0.0, 0.0, 0.0};  // this thread's interface fluxes
-      {
-        const double n0 = max_sel(fl[FN * W + sp], 0.05);
-        ux_own = fl[FPX * W + sp] / n0;
-        vz_own = fl[FPZ * W + sp] / n0;
-        if (t < TB - 1) {
-          const double n1 = max_sel(fl[FN * W + sp + 1], 0.05);
-          const double u1 = fl[FPX * W + sp + 1] / n1;
-          const double e = fct_eps(ux_own, u1, dtdx);
-          double nu;
-          fct_nu_mu(e, nu, mu_if);
+        // ---- A: velocities at sp, sp+1 (YM_Fluid.cu:3-11); interface sp+1/2:
+        // eps, nu, mu and the low-order fluxes of this half's variables
+        // (FCT_Sweeps.cu:88-98); half 0 also forms the px source at sp
+        // (YM_Fluid.cu:43-66, 71-80).
+        double vz_own, ux_own, mu_if = 0.0, sx = 0.0;
+        double Fo[3] = {0.0, 0.0, 0.0}, Do[3] = {0.0, 0.0, 0.0};  // this thread's interface fluxes
+        {
+          const double n0 = max_sel(fl[FN * W + sp], 0.05);
+          ux_own = fl[FPX * W + sp] / n0;
+          vz_own = fl[FPZ * W + sp] / n0;
+          if (t < TB - 1) {
+            const double n1 = max_sel(fl[FN * W + sp + 1], 0.05);
+            const double u1 = fl[FPX * W + sp + 1] / n1;
+            const double e = fct_eps(ux_own, u1, dtdx);
+            double nu;
+            fct_nu_mu(e, nu, mu_if);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+              const int k = k0 + j;
+              const double v0 = fl[k * W + sp], v1 = fl[k * W + sp + 1];
+              Fo[j] = 0.5 * e * (v0 + v1);
+              Do[j] = nu * (v1 - v0);
+              wb[(WB_F + k) * W + sp] = Fo[j];
+              wb[(WB_D + k) * W + sp] = Do[j];
+            }
+          }
+          if (half == 0 && t >= 1 && t < TB - 1) {
+            int ps = sp;  // at a wall the clamped ghost cells carry the edge cell's source
+            if (wall) {
+              const int xg = x0 - 4 + sp;
+              ps = (xg < 0 ? 0 : (xg >= nx ? nx - 1 : xg)) - (x0 - 4);
+            }
+            const double vz = (ps == sp) ? vz_own : fl[FPZ * W + ps] / max_sel(fl[FN * W + ps], 0.05);
+            double acc = 0.0;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              const double ex = 0.5 * (sb[(ST_EX + c) * W + ps] + sb[(ST_EX + c) * W + ps - 1]);
+              const double by = 0.25 * (sb[(ST_BY + c) * W + ps] + sb[(ST_BY + c) * W + ps - 1] +
+                                        sb[(ST_BYM + c) * W + ps] + sb[(ST_BYM + c) * W + ps - 1]);
+              const double term = fl[(FQ1 + c) * W + ps] * (ex + vz * by);
+              acc = (c == 0) ? term : acc + term;
+            }
+            sx = -acc;
+            if (warm) {
+              const double dndx = (fl[FN * W + ps + 1] - fl[FN * W + ps - 1]) / (2.0 * p.dx);
+              sx -= p.warm_T * dndx;
+            }
+          }
+        }
+        beam_bar(grp, TB);
+
+        // ---- B: lorhot / lnrhot at sp (FCT_Sweeps.cu:102-103), t in [1, TB-1).
+        double Lo[3] = {0.0, 0.0, 0.0}, Ln[3] = {0.0, 0.0, 0.0};  // this thread's lorhot, lnrhot
+        if (t >= 1 && t < TB - 1) {
 #pragma unroll
           for (int j = 0; j < 3; ++j) {
             const int k = k0 + j;
-            const double v0 = fl[k * W + sp], v1 = fl[k * W + sp + 1];
-            Fo[j] = 0.5 * e * (v0 + v1);
-            Do[j] = nu * (v1 - v0);
-            wb[(WB_F + k) * W + sp] = Fo[j];
-            wb[(WB_D + k) * W + sp] = Do[j];
+            const double v0 = fl[k * W + sp];
+            const double fd = Fo[j] - wb[(WB_F + k) * W + sp - 1];
+            const double dd = Do[j] - wb[(WB_D + k) * W + sp - 1];
+            const double lo = (k == FPX) ? v0 + dt * sx - fd : v0 - fd;
+            Lo[j] = lo;
+            Ln[j] = lo + dd;
+            wb[(WB_LOR + k) * W + sp] = lo;
+            wb[(WB_LNR + k) * W + sp] = Ln[j];
           }
         }
-        if (half == 0 && t >= 1 && t < TB - 1) {
-          int ps = sp;  // at a wall the clamped ghost cells carry the edge cell's source
-          if (wall) {
-            const int xg = x0 - 4 + sp;
-            ps = (xg < 0 ? 0 : (xg >= nx ? nx - 1 : xg)) - (x0 - 4);
-          }
-          const double vz = (ps == sp) ? vz_own : fl[FPZ * W + ps] / max_sel(fl[FN * W + ps], 0.05);
-          double acc = 0.0;
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const double ex = 0.5 * (sb[(ST_EX + c) * W + ps] + sb[(ST_EX + c) * W + ps - 1]);
-            const double by = 0.25 * (sb[(ST_BY + c) * W + ps] + sb[(ST_BY + c) * W + ps - 1] +
-                                      sb[(ST_BYM + c) * W + ps] + sb[(ST_BYM + c) * W + ps - 1]);
-            const double term = fl[(FQ1 + c) * W + ps] * (ex + vz * by);
-            acc = (c == 0) ? term : acc + term;
-          }
-          sx = -acc;
-          if (warm) {
-            const double dndx = (fl[FN * W + ps + 1] - fl[FN * W + ps - 1]) / (2.0 * p.dx);
-            sx -= p.warm_T * dndx;
-          }
-        }
-      }
-      beam_bar(grp, TB);
+        beam_bar(grp, TB);
 
-      // ---- B: lorhot / lnrhot at sp (FCT_Sweeps.cu:102-103), t in [1, TB-1).
-      double Lo[3] = {0.0, 0.0, 0.0}, Ln[3] = {0.0, 0.0, 0.0};  // this thread's lorhot, lnrhot
-      if (t >= 1 && t < TB - 1) {
+        // ---- C: antidiffusive flux and limiter at interface sp+1/2
+        // (FCT_Sweeps.cu:139-160), t in [2, TB-3).
+        double Fl[3] = {0.0, 0.0, 0.0};  // this thread's limited flux
+        if (t >= 2 && t < TB - 3) {
 #pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          const int k = k0 + j;
-          const double v0 = fl[k * W + sp];
-          const double fd = Fo[j] - wb[(WB_F + k) * W + sp - 1];
-          const double dd = Do[j] - wb[(WB_D + k) * W + sp - 1];
-          const double lo = (k == FPX) ? v0 + dt * sx - fd : v0 - fd;
-          Lo[j] = lo;
-          Ln[j] = lo + dd;
-          wb[(WB_LOR + k) * W + sp] = lo;
-          wb[(WB_LNR + k) * W + sp] = Ln[j];
-        }
-      }
-      beam_bar(grp, TB);
-
-      // ---- C: antidiffusive flux and limiter at interface sp+1/2
-      // (FCT_Sweeps.cu:139-160), t in [2, TB-3).
-      double Fl[3] = {0.0, 0.0, 0.0};  // this thread's limited flux
-      if (t >= 2 && t < TB - 3) {
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          const int k = k0 + j;
-          const double* lor = wb + (WB_LOR + k) * W;
-          const double* lnr = wb + (WB_LNR + k) * W;
-          const double l1 = lnr[sp + 1];
-          const double fad = mu_if * (lor[sp + 1] - Lo[j]);
-          Fl[j] = fct_limit_sel(fad, Ln[j] - lnr[sp - 1], l1 - Ln[j], lnr[sp + 2] - l1);
-          wb[(WB_FLIM + k) * W + sp] = Fl[j];
-        }
-      }
-      beam_bar(grp, TB);
-
-      // ---- D: x-swept values of the own column, z-sources, z-pipeline.
-      if (zthread) {
-        double Vx[3], S[3];
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          const int k = k0 + j;
-          Vx[j] = Ln[j] - (Fl[j] - wb[(WB_FLIM + k) * W + sp - 1]);
-        }
-        const double vz = vz_own;
-        const double q1 = fl[FQ1 * W + sp], q2 = fl[FQ2 * W + sp], q3 = fl[FQ3 * W + sp];
-        if (half == 0) {
-          // the pz source of row r-1, formed by the Q group last row
-          S[0] = 0.0;
-          S[1] = 0.0;
-          S[2] = 0.0;
-          zp.S1[2] = wb[(WB_SZ + ((r - 1) & 1)) * W + sp];
-        } else {
-          // YM_Fluid.cu:67 (src.pz) and :76-79 (warm closure), for the other group
-          const double vx = ux_own;
-          double by[3], ezn[3];
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            by[c] = 0.25 * (sb[(ST_BY + c) * W + sp] + sb[(ST_BY + c) * W + sp - 1] + sb[(ST_BYM + c) * W + sp] +
-                            sb[(ST_BYM + c) * W + sp - 1]);
-            ezn[c] = 0.5 * (sb[(ST_EZ + c) * W + sp] + sb[(ST_EZM + c) * W + sp]);
+          for (int j = 0; j < 3; ++j) {
+            const int k = k0 + j;
+            const double* lor = wb + (WB_LOR + k) * W;
+            const double* lnr = wb + (WB_LNR + k) * W;
+            const double l1 = lnr[sp + 1];
+            const double fad = mu_if * (lor[sp + 1] - Lo[j]);
+            Fl[j] = fct_limit_sel(fad, Ln[j] - lnr[sp - 1], l1 - Ln[j], lnr[sp + 2] - l1);
+            wb[(WB_FLIM + k) * W + sp] = Fl[j];
           }
-          double sz = -(q1 * (ezn[0] - vx * by[0]) + q2 * (ezn[1] - vx * by[1]) + q3 * (ezn[2] - vx * by[2]));
-          if (warm) {
-            const double dndz = (sb[(ST_NZP + beam) * W + sp] - sb[(ST_NZM + beam) * W + sp]) / (2.0 * p.dz);
-            sz -= p.warm_T * dndz;
-          }
-          wb[(WB_SZ + (r & 1)) * W + sp] = sz;
-          // YM_Fluid.cu:99-107 (colour precession)
-          double azn[3];
-#pragma unroll
-          for (int c = 0; c < 3; ++c) azn[c] = 0.5 * (sb[(ST_AZ + c) * W + sp] + sb[(ST_AZM + c) * W + sp]);
-          S[0] = p.alpha * vz * (q2 * azn[2] - q3 * azn[1]);
-          S[1] = p.alpha * vz * (q3 * azn[0] - q1 * azn[2]);
-          S[2] = p.alpha * vz * (q1 * azn[1] - q2 * azn[0]);
         }
+        beam_bar(grp, TB);
 
-        const double e = fct_eps(zp.U1, vz, dtdz);
-        double nu, mu;
-        fct_nu_mu(e, nu, mu);
-        double outv[3];
+        // ---- D: x-swept values of the own column, z-sources, z-pipeline.
+        if (zthread) {
+          double Vx[3], S[3];
 #pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          const bool has_src = (half == 1) || (j == 2);  // pz and Q1..Q3 carry z-sources
-          const double fR = 0.5 * e * (zp.V1[j] + Vx[j]);
-          const double dR = nu * (Vx[j] - zp.V1[j]);
-          const double lo = has_src ? zp.V1[j] + dt * zp.S1[j] - (fR - zp.f1[j]) : zp.V1[j] - (fR - zp.f1[j]);
-          const double ln = lo + (dR - zp.d1[j]);
-          const double fad = zp.mu1 * (lo - zp.L2[j]);
-          const double flim = fct_limit_sel(zp.A2[j], zp.N3[j] - zp.N4[j], zp.N2[j] - zp.N3[j], ln - zp.N2[j]);
-          outv[j] = zp.N3[j] - (flim - zp.F3[j]);
-          zp.V1[j] = Vx[j];
-          zp.S1[j] = S[j];
-          zp.f1[j] = fR;
-          zp.d1[j] = dR;
-          zp.L2[j] = lo;
-          zp.N4[j] = zp.N3[j];
-          zp.N3[j] = zp.N2[j];
-          zp.N2[j] = ln;
-          zp.A2[j] = fad;
-          zp.F3[j] = flim;
-        }
-        zp.U1 = vz;
-        zp.mu1 = mu;
-        const int o = r - 3;
-        if (owner && o >= zs && o < ze) {
-          // YM_Fluid.cu:20-29 (density floor, wall momentum)
+          for (int j = 0; j < 3; ++j) {
+            const int k = k0 + j;
+            Vx[j] = Ln[j] - (Fl[j] - wb[(WB_FLIM + k) * W + sp - 1]);
+          }
+          const double vz = vz_own;
+          const double q1 = fl[FQ1 * W + sp], q2 = fl[FQ2 * W + sp], q3 = fl[FQ3 * W + sp];
           if (half == 0) {
-            if (outv[0] < 0.05) outv[0] = 0.05;
-            if (wall && (x_own == 0 || x_own == nx - 1)) outv[1] = 0.0;
-          }
-          double* const* dst = beam ? out.b : out.a;
-          const size_t gi = idx2(x_own, o, nx);
-          if (dbg_ok(x_own >= 0 && x_own < nx && o >= 0 && o < nz && sp >= 1 && sp + 2 < W, T.err)) {
+            // the pz source of row r-1, formed by the Q group last row
+            S[0] = 0.0;
+            S[1] = 0.0;
+            S[2] = 0.0;
+            zp.S1[2] = wb[(WB_SZ + ((r - 1) & 1)) * W + sp];
+          } else {
+            // YM_Fluid.cu:67 (src.pz) and :76-79 (warm closure), for the other group
+            const double vx = ux_own;
+            double by[3], ezn[3];
 #pragma unroll
-            for (int j = 0; j < 3; ++j) dst[k0 + j][gi] = outv[j];
+            for (int c = 0; c < 3; ++c) {
+              by[c] = 0.25 * (sb[(ST_BY + c) * W + sp] + sb[(ST_BY + c) * W + sp - 1] + sb[(ST_BYM + c) * W + sp] +
+                              sb[(ST_BYM + c) * W + sp - 1]);
+              ezn[c] = 0.5 * (sb[(ST_EZ + c) * W + sp] + sb[(ST_EZM + c) * W + sp]);
+            }
+            double sz = -(q1 * (ezn[0] - vx * by[0]) + q2 * (ezn[1] - vx * by[1]) + q3 * (ezn[2] - vx * by[2]));
+            if (warm) {
+              const double dndz = (sb[(ST_NZP + beam) * W + sp] - sb[(ST_NZM + beam) * W + sp]) / (2.0 * p.dz);
+              sz -= p.warm_T * dndz;
+            }
+            wb[(WB_SZ + (r & 1)) * W + sp] = sz;
+            // YM_Fluid.cu:99-107 (colour precession)
+            double azn[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) azn[c] = 0.5 * (sb[(ST_AZ + c) * W + sp] + sb[(ST_AZM + c) * W + sp]);
+            S[0] = p.alpha * vz * (q2 * azn[2] - q3 * azn[1]);
+            S[1] = p.alpha * vz * (q3 * azn[0] - q1 * azn[2]);
+            S[2] = p.alpha * vz * (q1 * azn[1] - q2 * azn[0]);
+          }
+
+          const double e = fct_eps(zp.U1, vz, dtdz);
+          double nu, mu;
+          fct_nu_mu(e, nu, mu);
+          double outv[3];
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const bool has_src = (half == 1) || (j == 2);  // pz and Q1..Q3 carry z-sources
+            const double fR = 0.5 * e * (zp.V1[j] + Vx[j]);
+            const double dR = nu * (Vx[j] - zp.V1[j]);
+            const double lo = has_src ? zp.V1[j] + dt * zp.S1[j] - (fR - zp.f1[j]) : zp.V1[j] - (fR - zp.f1[j]);
+            const double ln = lo + (dR - zp.d1[j]);
+            const double fad = zp.mu1 * (lo - zp.L2[j]);
+            const double flim = fct_limit_sel(zp.A2[j], zp.N3[j] - zp.N4[j], zp.N2[j] - zp.N3[j], ln - zp.N2[j]);
+            outv[j] = zp.N3[j] - (flim - zp.F3[j]);
+            zp.V1[j] = Vx[j];
+            zp.S1[j] = S[j];
+            zp.f1[j] = fR;
+            zp.d1[j] = dR;
+            zp.L2[j] = lo;
+            zp.N4[j] = zp.N3[j];
+            zp.N3[j] = zp.N2[j];
+            zp.N2[j] = ln;
+            zp.A2[j] = fad;
+            zp.F3[j] = flim;
+          }
+          zp.U1 = vz;
+          zp.mu1 = mu;
+          const int o = r - 3;
+          if (owner && o >= zs && o < ze) {
+            // YM_Fluid.cu:20-29 (density floor, wall momentum)
+            if (half == 0) {
+              if (outv[0] < 0.05) outv[0] = 0.05;
+              if (wall && (x_own == 0 || x_own == nx - 1)) outv[1] = 0.0;
+            }
+            double* const* dst = beam ? out.b : out.a;
+            const size_t gi = idx2(x_own, o, nx);
+            if (dbg_ok(x_own >= 0 && x_own < nx && o >= 0 && o < nz && sp >= 1 && sp + 2 < W, T.err)) {
+#pragma unroll
+              for (int j = 0; j < 3; ++j) dst[k0 + j][gi] = outv[j];
+            }
           }
         }
       }
-    }
+    };
+    if (half == 0) rows(HalfC<0>{});
+    else rows(HalfC<1>{});
     if (!bulk) cp_async_wait<0>();
   }
 }
