@@ -464,7 +464,7 @@ def main() -> int:
         line["served"] = served_rate(args, dev, args.served_seconds)
     if world == 1 and not args.no_config0:
         line["config0"] = config0_rate(dev)
-    if rank == 0 and not args.no_cpu_baseline:
+    if world == 1 and not args.no_cpu_baseline:  # a host-core figure, taken at N = 1 only
         line["cpu_baseline"] = cpu_oracle_rate(args.workload, 1, min_seconds=10.0)
         line["cpu_baselines"] = cpu_baselines()
     if rank == 0:
