@@ -43,7 +43,7 @@ def lookup(nx: int, nz: int, filtered: bool):
 
 def candidates(nx: int, nz: int):
     tbs = [tb for tb in (32, 64, 128) if nx >= tb - 6]
-    segs = sorted({s for s in (16, 32, 64, 128) if s <= max(16, nz)})
+    segs = sorted({s for s in (1, 16, 32, 64, 128) if s <= max(16, nz)})
     return [(tb, s) for tb in tbs for s in segs]
 
 

@@ -231,7 +231,12 @@ int pick_segment(int nz, int nstrips, int grid) {
   return best_seg;
 }
 
-constexpr int kFctSegment = 16;
+// One-row segments: a CTA's contiguous block then ends at any row, so the
+// blocks differ by at most one row (at 1024 x 2048 on B200 the step took
+// 0.523 ms against 0.529 ms with 16-row segments, 7.38 against 7.40 ms at
+// 4096 x 8192).  Maxwell keeps round-robin segments: its contiguous form
+// measured slower (7.49 ms).
+constexpr int kFctSegment = 1;
 
 void choose_launch_shape(ymkh_ctx* c) {
   cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);

@@ -498,12 +498,13 @@ static cudaError_t prepare_fct_t() {
                               (int)fct_smem_bytes<TB>(NST));
 }
 
-// Stage ring depth per strip width (rows in flight = NST - 1).  Measured at
-// 4096 x 8192 on B200 with 128-wide strips: 6.40 ms with 2 stages against
-// 6.55 ms with 3 or 4.
+// Stage ring depth (rows in flight = NST - 1).  Measured on B200 with
+// 128-wide strips, step ms at 4096 x 8192 / 1024 x 2048: 7.38 / 0.522 with
+// 2 stages, 7.18 / 0.505 with 3, 7.06 / 0.497 with 4 (206 KB of shared
+// memory; 5 stages do not fit).  64-wide strips run 2 CTAs of 4 stages per SM.
 template <int TB>
 constexpr int fct_nst() {
-  return TB >= 128 ? 2 : 4;
+  return 4;
 }
 
 int fct_nstrips(int nx, int tb) { return (nx + (tb - 6) - 1) / (tb - 6); }

@@ -284,8 +284,8 @@ STRIP_CASES = {
 
 @pytest.mark.parametrize("name", sorted(STRIP_CASES))
 def test_fct_strip_widths_identical(cuda, name):
-    """The fused FCT with 32-, 64- and 128-wide strips (short and long
-    segments) and the split form give the same state bit for bit after 3
+    """The fused FCT with 32-, 64- and 128-wide strips (one-row, short and
+    long segments) and the split form give the same state bit for bit after 3
     steps: TMA rows and per-element rows (walls), warm_T rows, ragged
     strips."""
     from kh_simulations_b200 import _lib
@@ -296,7 +296,7 @@ def test_fct_strip_widths_identical(cuda, name):
     if name.startswith("wall"):
         text = text.replace("run_mode = 6", "run_mode = 0")
     out = {}
-    for form in ((32, 8), (64, 16), (128, 16), (128, 5), "split"):
+    for form in ((32, 8), (64, 16), (64, 1), (128, 16), (128, 5), (128, 1), "split"):
         r = KHRun(loads(text, name))
         r.init()
         if form == "split":
