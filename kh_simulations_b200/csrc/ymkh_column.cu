@@ -107,7 +107,71 @@ __global__ void zmean_kernel(const __grid_constant__ ArrayList a15, int nx, int 
   }
 }
 
+// Power-of-two NZ = 32 M: one CTA per (32 columns, array), warp l holding the
+// rows z = l + 32 j of its lane's column, so every load is one coalesced row
+// segment.  The halving tree pairs z with z + NZ/2, then z + NZ/4, ...: its
+// levels down to stride 32 stay inside a residue class z mod 32, where they
+// form the same halving tree over j; each thread sums its class in that order
+// with a pairwise binary counter over the leaves in bit-reversed j order
+// (T(y) = T(y_even) + T(y_odd)), and the last five levels (strides 16 .. 1)
+// are a shuffle tree over the 32 class sums.  The sum is therefore the
+// halving tree's, bit for bit; the columns are then re-read (mostly from L2)
+// and the mean subtracted.
+template <int LOGM>
+__global__ void __launch_bounds__(1024) zmean_p2_kernel(const __grid_constant__ ArrayList a15, int nx) {
+  constexpr int M = 1 << LOGM;
+  __shared__ double part[32][33];
+  __shared__ double mean[32];
+  const int lane = threadIdx.x & 31, l = threadIdx.x >> 5;
+  const int x = blockIdx.x * 32 + lane;
+  double* g = a15.p[blockIdx.y];
+  const bool in = x < nx;
+  double st[LOGM + 1];
+#pragma unroll
+  for (int jj = 0; jj < M; ++jj) {
+    int j = 0;
+#pragma unroll
+    for (int b = 0; b < LOGM; ++b) j |= ((jj >> b) & 1) << (LOGM - 1 - b);
+    double carry = in ? g[(size_t)(l + 32 * j) * nx + x] : 0.0;
+    int k = 0;
+#pragma unroll
+    for (int b = 0; b < LOGM; ++b) {
+      if (((jj >> b) & 1) == 0) break;
+      carry = st[b] + carry;
+      k = b + 1;
+    }
+    st[k] = carry;
+  }
+  part[l][lane] = st[LOGM];
+  __syncthreads();
+  {
+    double v = part[lane][l];  // warp l: column l of the tile, lane = residue class
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, d);
+    if (lane == 0) mean[l] = v * (1.0 / (double)(32 * M));
+  }
+  __syncthreads();
+  if (in) {
+    const double mu = mean[lane];
+#pragma unroll 8
+    for (int j = 0; j < M; ++j) {
+      const size_t gi = (size_t)(l + 32 * j) * nx + x;
+      g[gi] -= mu;
+    }
+  }
+}
+
 cudaError_t launch_zmean(const ArrayList& a15, int nx, int nz, cudaStream_t s) {
+  const dim3 g32((nx + 31) / 32, 15);
+  switch (nz) {
+    case 128: zmean_p2_kernel<2><<<g32, 1024, 0, s>>>(a15, nx); return cudaGetLastError();
+    case 256: zmean_p2_kernel<3><<<g32, 1024, 0, s>>>(a15, nx); return cudaGetLastError();
+    case 512: zmean_p2_kernel<4><<<g32, 1024, 0, s>>>(a15, nx); return cudaGetLastError();
+    case 1024: zmean_p2_kernel<5><<<g32, 1024, 0, s>>>(a15, nx); return cudaGetLastError();
+    case 2048: zmean_p2_kernel<6><<<g32, 1024, 0, s>>>(a15, nx); return cudaGetLastError();
+    case 4096: zmean_p2_kernel<7><<<g32, 1024, 0, s>>>(a15, nx); return cudaGetLastError();
+    default: break;
+  }
   const size_t smem = (size_t)nz * ZM_CX * sizeof(double);
   dim3 grid((nx + ZM_CX - 1) / ZM_CX, 15);
   zmean_kernel<<<grid, 256, smem, s>>>(a15, nx, nz);
