@@ -5,10 +5,9 @@
 //   FCT x+z sweeps of both beams, density floor   -> fct_fused_kernel
 //   currents, Ampère, potential, Faraday          -> maxwell_fused_kernel
 //   sponge, xi_cut                                -> sponge_xicut_kernel
-//   z-mean removal                                -> zmean_kernel
+//   z-mean removal and colour-1 EM zeroing        -> zmean_p2_kernel / zmean_kernel
 //   DFT kz bands on the 21 filtered arrays        -> band_coef / band_apply
 //   z-hyperdiffusion                              -> hyperdiff_kernel
-//   colour-1 EM zeroing                           -> cudaMemsetAsync
 // The sources of stage 7 are recomputed inside the next FCT launch.
 //
 // The stencil kernels read start-of-step values of neighbouring tiles, so
@@ -337,6 +336,13 @@ int flush_desc(ymkh_ctx* c, cudaStream_t s) {
   return 0;
 }
 
+// list21 without its first k arrays
+ArrayList drop_front(const ArrayList& l, int k) {
+  ArrayList r{};
+  for (int i = 0; i + k < 24; ++i) r.p[i] = l.p[i + k];
+  return r;
+}
+
 ArrayList list21(const State& s) {
   ArrayList l{};
   double* v[21] = {s.f[BY1], s.f[EX1], s.f[EZ1], s.f[BY2], s.f[BY3], s.f[EX2], s.f[EX3],
@@ -365,17 +371,30 @@ int post_stages(ymkh_ctx* c, const State& out, cudaStream_t s) {
   mark(c, ST_POINTWISE, s);
   if (c->prm.xi_sponge > 0.0) { CK(launch_sponge_xicut(list12(out), c->sp, 0, s), "sponge"); g_launches++; }
   if (c->prm.xi_cut > 0.0) { CK(launch_sponge_xicut(list12(out), c->sp, 1, s), "xi_cut"); g_launches++; }
+  // With suppress_kz0 the step ends by zeroing By1, Ex1 and Ez1, the first
+  // three arrays of list21 (main_ym.cu:443-447).  The z-mean and the band
+  // filters treat every array on its own and hyperdiffusion does not touch
+  // colour 1, so the z-mean launch zeroes those three and the later stages
+  // skip them: the state after the step is the same bit for bit.
+  const int skip = c->prm.suppress_kz0 ? 3 : 0;
+  const ArrayList l21 = list21(out);
+  const ArrayList filt = drop_front(l21, skip);
   mark(c, ST_ZMEAN, s);
-  if (c->prm.suppress_kz0) { CK(launch_zmean(list21(out), c->nx, c->nz, s), "zmean"); g_launches++; }
+  if (c->prm.suppress_kz0) {
+    ArrayList zl = filt;  // 12 arrays lose their z-mean, then By1, Ex1, Ez1 are zeroed
+    for (int i = 0; i < 3; ++i) zl.p[12 + i] = l21.p[i];
+    CK(launch_zmean(zl, 12, 3, c->nx, c->nz, s), "zmean");
+    g_launches++;
+  }
   mark(c, ST_BANDS, s);
   const double inv2 = (double)(2.0f / (float)c->nz);
   for (int b = 0; b < c->nb; ++b) {
     if (c->prm.filter_engine == YMKH_FILTER_TF32X3) {
-      CK(launch_band_tf32(list21(out), 21, c->tfb[b], c->tfs, c->nx, c->nz, 2.0f / (float)c->nz, c->derr, s),
+      CK(launch_band_tf32(filt, 21 - skip, c->tfb[b], c->tfs, c->nx, c->nz, 2.0f / (float)c->nz, c->derr, s),
          "band filter (TF32 tensor cores)");
       g_launches += 3;
     } else {
-      CK(launch_band(list21(out), 21, c->W[b], c->J[b], c->J[b], c->coef, c->nx, c->nz, inv2, s), "band filter");
+      CK(launch_band(filt, 21 - skip, c->W[b], c->J[b], c->J[b], c->coef, c->nx, c->nz, inv2, s), "band filter");
       g_launches += 2;
     }
   }
@@ -384,13 +403,7 @@ int post_stages(ymkh_ctx* c, const State& out, cudaStream_t s) {
     CK(launch_hyperdiff(list12(out), c->nx, c->nz, c->prm.hyp_diff_coeff, s), "hyperdiffusion");
     g_launches++;
   }
-  mark(c, ST_ZERO, s);
-  if (c->prm.suppress_kz0) {
-    const size_t bytes = c->N * sizeof(double);
-    CK(cudaMemsetAsync(out.f[BY1], 0, bytes, s), "zero By1");
-    CK(cudaMemsetAsync(out.f[EX1], 0, bytes, s), "zero Ex1");
-    CK(cudaMemsetAsync(out.f[EZ1], 0, bytes, s), "zero Ez1");
-  }
+  mark(c, ST_ZERO, s);  // colour-1 zeroing: done by the z-mean launch above
   mark(c, ST_COUNT, s);
   return 0;
 }

@@ -81,13 +81,23 @@ cudaError_t launch_sponge_xicut(const ArrayList& a12, const StepParams& p, int c
 }
 
 // -------------------------------------------------------------- z-mean
+// Arrays [0, nmean) lose their z-mean; arrays [nmean, gridDim.y) are set to
+// zero (the colour-1 fields, which the step zeroes once the z-mean is done:
+// ymgpu2d/main_ym.cu:443-447; no stage in between reads or writes them).
 // One CTA per (4 columns, array).  The column sum uses the reference's
 // halving tree (YM_Physics.cu:301-308) so the mean is bit-identical.
 constexpr int ZM_CX = 4;
-__global__ void zmean_kernel(const __grid_constant__ ArrayList a15, int nx, int nz) {
+__global__ void zmean_kernel(const __grid_constant__ ArrayList arrs, int nx, int nz, int nmean) {
   extern __shared__ double sm[];  // [nz][ZM_CX]
   const int x0 = blockIdx.x * ZM_CX;
-  double* g = a15.p[blockIdx.y];
+  double* g = arrs.p[blockIdx.y];
+  if ((int)blockIdx.y >= nmean) {
+    for (int i = threadIdx.x; i < nz * ZM_CX; i += blockDim.x) {
+      const int z = i / ZM_CX, c = i - z * ZM_CX;
+      if (x0 + c < nx) g[idx2(x0 + c, z, nx)] = 0.0;
+    }
+    return;
+  }
   for (int i = threadIdx.x; i < nz * ZM_CX; i += blockDim.x) {
     const int z = i / ZM_CX, c = i - z * ZM_CX;
     sm[i] = (x0 + c < nx) ? g[idx2(x0 + c, z, nx)] : 0.0;
@@ -118,14 +128,20 @@ __global__ void zmean_kernel(const __grid_constant__ ArrayList a15, int nx, int 
 // halving tree's, bit for bit; the columns are then re-read (mostly from L2)
 // and the mean subtracted.
 template <int LOGM>
-__global__ void __launch_bounds__(1024) zmean_p2_kernel(const __grid_constant__ ArrayList a15, int nx) {
+__global__ void __launch_bounds__(1024) zmean_p2_kernel(const __grid_constant__ ArrayList arrs, int nx, int nmean) {
   constexpr int M = 1 << LOGM;
   __shared__ double part[32][33];
   __shared__ double mean[32];
   const int lane = threadIdx.x & 31, l = threadIdx.x >> 5;
   const int x = blockIdx.x * 32 + lane;
-  double* g = a15.p[blockIdx.y];
+  double* g = arrs.p[blockIdx.y];
   const bool in = x < nx;
+  if ((int)blockIdx.y >= nmean) {  // an array the step zeroes (zmean_kernel)
+    if (in)
+#pragma unroll 8
+      for (int j = 0; j < M; ++j) g[(size_t)(l + 32 * j) * nx + x] = 0.0;
+    return;
+  }
   double st[LOGM + 1];
 #pragma unroll
   for (int jj = 0; jj < M; ++jj) {
@@ -161,20 +177,21 @@ __global__ void __launch_bounds__(1024) zmean_p2_kernel(const __grid_constant__ 
   }
 }
 
-cudaError_t launch_zmean(const ArrayList& a15, int nx, int nz, cudaStream_t s) {
-  const dim3 g32((nx + 31) / 32, 15);
+cudaError_t launch_zmean(const ArrayList& arrs, int nmean, int nzero, int nx, int nz, cudaStream_t s) {
+  const int narr = nmean + nzero;
+  const dim3 g32((nx + 31) / 32, narr);
   switch (nz) {
-    case 128: zmean_p2_kernel<2><<<g32, 1024, 0, s>>>(a15, nx); return cudaGetLastError();
-    case 256: zmean_p2_kernel<3><<<g32, 1024, 0, s>>>(a15, nx); return cudaGetLastError();
-    case 512: zmean_p2_kernel<4><<<g32, 1024, 0, s>>>(a15, nx); return cudaGetLastError();
-    case 1024: zmean_p2_kernel<5><<<g32, 1024, 0, s>>>(a15, nx); return cudaGetLastError();
-    case 2048: zmean_p2_kernel<6><<<g32, 1024, 0, s>>>(a15, nx); return cudaGetLastError();
-    case 4096: zmean_p2_kernel<7><<<g32, 1024, 0, s>>>(a15, nx); return cudaGetLastError();
+    case 128: zmean_p2_kernel<2><<<g32, 1024, 0, s>>>(arrs, nx, nmean); return cudaGetLastError();
+    case 256: zmean_p2_kernel<3><<<g32, 1024, 0, s>>>(arrs, nx, nmean); return cudaGetLastError();
+    case 512: zmean_p2_kernel<4><<<g32, 1024, 0, s>>>(arrs, nx, nmean); return cudaGetLastError();
+    case 1024: zmean_p2_kernel<5><<<g32, 1024, 0, s>>>(arrs, nx, nmean); return cudaGetLastError();
+    case 2048: zmean_p2_kernel<6><<<g32, 1024, 0, s>>>(arrs, nx, nmean); return cudaGetLastError();
+    case 4096: zmean_p2_kernel<7><<<g32, 1024, 0, s>>>(arrs, nx, nmean); return cudaGetLastError();
     default: break;
   }
   const size_t smem = (size_t)nz * ZM_CX * sizeof(double);
-  dim3 grid((nx + ZM_CX - 1) / ZM_CX, 15);
-  zmean_kernel<<<grid, 256, smem, s>>>(a15, nx, nz);
+  dim3 grid((nx + ZM_CX - 1) / ZM_CX, narr);
+  zmean_kernel<<<grid, 256, smem, s>>>(arrs, nx, nz, nmean);
   return cudaGetLastError();
 }
 

@@ -179,7 +179,8 @@ cudaError_t prepare_maxwell();
 int maxwell_ctas_per_sm();
 cudaError_t launch_sponge_xicut(const ArrayList& a12, const StepParams& p, int cut, cudaStream_t s);
 cudaError_t prepare_column(int nz);
-cudaError_t launch_zmean(const ArrayList& a15, int nx, int nz, cudaStream_t s);
+// The z-mean of arrs[0, nmean) removed and arrs[nmean, nmean + nzero) zeroed, in one launch.
+cudaError_t launch_zmean(const ArrayList& arrs, int nmean, int nzero, int nx, int nz, cudaStream_t s);
 cudaError_t launch_hyperdiff(const ArrayList& a12, int nx, int nz, double mu, cudaStream_t s);
 cudaError_t launch_band(const ArrayList& arrs, int narr, const double* W, int ldw, int J, double* C, int nx, int nz,
                         double inv2, cudaStream_t s);
