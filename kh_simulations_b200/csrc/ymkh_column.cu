@@ -221,7 +221,46 @@ __global__ void hyperdiff_kernel(const __grid_constant__ ArrayList a12, int nx, 
   }
 }
 
+// NZ a multiple of 32 (at least 64): one 1024-thread CTA per (32 columns,
+// array); lane c holds column c and warp w the rows [w L, (w+1) L), L = NZ/32,
+// so every access is a coalesced 256-byte row segment.  Each warp first reads
+// the two rows on either side of its segment (periodic in z), then the CTA
+// synchronises, and each warp updates its own rows in place from a five-row
+// window of values read before any write: every stencil sees the values from
+// before the update, as hyperdiff_kernel's shared copy gives, with the same
+// arithmetic, so the result is the same bit for bit.
+__global__ void __launch_bounds__(1024) hyperdiff_seg_kernel(const __grid_constant__ ArrayList a12, int nx, int nz,
+                                                             double mu) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int x = blockIdx.x * 32 + lane;
+  const bool in = x < nx;
+  double* g = a12.p[blockIdx.y];
+  const int L = nz >> 5, z0 = w * L;
+  auto at = [&](int z) -> double {
+    z = z < 0 ? z + nz : (z >= nz ? z - nz : z);
+    return in ? g[(size_t)z * nx + x] : 0.0;
+  };
+  const double h0 = at(z0 - 2), h1 = at(z0 - 1);        // rows below the segment
+  const double t0 = at(z0 + L), t1 = at(z0 + L + 1);    // rows above it
+  __syncthreads();  // every warp holds its neighbours' rows before any write
+  double w0 = h0, w1 = h1, w2 = at(z0), w3 = at(z0 + 1);
+#pragma unroll 4
+  for (int k = 0; k < L; ++k) {
+    const double w4 = (k + 2 < L) ? at(z0 + k + 2) : (k + 2 == L ? t0 : t1);
+    const double d4 = w0 - 4.0 * w1 + 6.0 * w2 - 4.0 * w3 + w4;
+    if (in) g[(size_t)(z0 + k) * nx + x] = w2 - mu * d4;
+    w0 = w1;
+    w1 = w2;
+    w2 = w3;
+    w3 = w4;
+  }
+}
+
 cudaError_t launch_hyperdiff(const ArrayList& a12, int nx, int nz, double mu, cudaStream_t s) {
+  if (nz % 32 == 0 && nz >= 64) {
+    hyperdiff_seg_kernel<<<dim3((nx + 31) / 32, 12), 1024, 0, s>>>(a12, nx, nz, mu);
+    return cudaGetLastError();
+  }
   const size_t smem = (size_t)nz * HD_CX * sizeof(double);
   dim3 grid((nx + HD_CX - 1) / HD_CX, 12);
   hyperdiff_kernel<<<grid, 256, smem, s>>>(a12, nx, nz, mu);
