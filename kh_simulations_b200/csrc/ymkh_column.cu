@@ -87,6 +87,7 @@ cudaError_t launch_sponge_xicut(const ArrayList& a12, const StepParams& p, int c
 // One CTA per (4 columns, array).  The column sum uses the reference's
 // halving tree (YM_Physics.cu:301-308) so the mean is bit-identical.
 constexpr int ZM_CX = 4;
+constexpr size_t kColumnSmemMax = 200 * 1024;  // shared memory of the staged-column kernels
 __global__ void zmean_kernel(const __grid_constant__ ArrayList arrs, int nx, int nz, int nmean) {
   extern __shared__ double sm[];  // [nz][ZM_CX]
   const int x0 = blockIdx.x * ZM_CX;
@@ -187,9 +188,11 @@ cudaError_t launch_zmean(const ArrayList& arrs, int nmean, int nzero, int nx, in
     case 1024: zmean_p2_kernel<5><<<g32, 1024, 0, s>>>(arrs, nx, nmean); return cudaGetLastError();
     case 2048: zmean_p2_kernel<6><<<g32, 1024, 0, s>>>(arrs, nx, nmean); return cudaGetLastError();
     case 4096: zmean_p2_kernel<7><<<g32, 1024, 0, s>>>(arrs, nx, nmean); return cudaGetLastError();
+    case 8192: zmean_p2_kernel<8><<<g32, 1024, 0, s>>>(arrs, nx, nmean); return cudaGetLastError();
     default: break;
   }
   const size_t smem = (size_t)nz * ZM_CX * sizeof(double);
+  if (smem > kColumnSmemMax) return cudaErrorInvalidValue;  // NZ > 6400 without a coalesced form
   dim3 grid((nx + ZM_CX - 1) / ZM_CX, narr);
   zmean_kernel<<<grid, 256, smem, s>>>(arrs, nx, nz, nmean);
   return cudaGetLastError();
@@ -262,20 +265,26 @@ cudaError_t launch_hyperdiff(const ArrayList& a12, int nx, int nz, double mu, cu
     return cudaGetLastError();
   }
   const size_t smem = (size_t)nz * HD_CX * sizeof(double);
+  if (smem > kColumnSmemMax) return cudaErrorInvalidValue;  // NZ > 6400 and not a multiple of 32
   dim3 grid((nx + HD_CX - 1) / HD_CX, 12);
   hyperdiff_kernel<<<grid, 256, smem, s>>>(a12, nx, nz, mu);
   return cudaGetLastError();
 }
 
-// Column kernels keep a block of whole columns in shared memory.
-// The dynamic shared-memory limit is a property of the kernel, shared by
-// every run in the process: it only ever grows (to the largest NZ seen), so
-// a run with a smaller NZ never lowers it under a larger resident run.
+// The staged-column kernels (zmean_kernel, hyperdiff_kernel) keep a block of
+// whole columns in shared memory.  The dynamic shared-memory limit is a
+// property of the kernel, shared by every run in the process: it only ever
+// grows (to the largest NZ seen), so a run with a smaller NZ never lowers it
+// under a larger resident run.  Above kColumnSmemMax (NZ > 6400) nothing is
+// set: such runs use the coalesced kernels, and a stage that would need a
+// staged kernel there fails at its launch.
+size_t column_smem(int nz) { return (size_t)nz * (ZM_CX > HD_CX ? ZM_CX : HD_CX) * sizeof(double); }
+
 cudaError_t prepare_column(int nz) {
   static std::mutex mu;
   static size_t granted[64];  // per device
-  const size_t smem = (size_t)nz * (ZM_CX > HD_CX ? ZM_CX : HD_CX) * sizeof(double);
-  if (smem > 200 * 1024) return cudaErrorInvalidValue;
+  const size_t smem = column_smem(nz);
+  if (smem > kColumnSmemMax) return cudaSuccess;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(mu);
