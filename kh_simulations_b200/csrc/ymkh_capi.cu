@@ -336,7 +336,7 @@ int flush_desc(ymkh_ctx* c, cudaStream_t s) {
   return 0;
 }
 
-// list21 without its first k arrays
+// The list l without its first k arrays.
 ArrayList drop_front(const ArrayList& l, int k) {
   ArrayList r{};
   for (int i = 0; i + k < 24; ++i) r.p[i] = l.p[i + k];
